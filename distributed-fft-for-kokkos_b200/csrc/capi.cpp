@@ -1,0 +1,284 @@
+// extern "C" entry points declared in include/dfft.h.  Every call catches
+// the planner's exceptions and turns them into a dfft_status plus a
+// thread-local message (the reference throws std::runtime_error via
+// KOKKOSFFT_THROW_IF; nothing may unwind across a C ABI).
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/dfft.h"
+#include "plan.hpp"
+
+struct dfft_plan_s {
+  dfft::Plan* impl;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+dfft_status set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return static_cast<dfft_status>(code);
+}
+
+template <typename F>
+dfft_status guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return DFFT_SUCCESS;
+  } catch (const dfft::Error& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return set_error(DFFT_ERROR_ALLOC, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_error(DFFT_ERROR_INTERNAL, e.what());
+  } catch (...) {
+    return set_error(DFFT_ERROR_INTERNAL, "unknown error");
+  }
+}
+
+dfft::PlanDesc to_desc(const dfft_plan_desc* d) {
+  if (!d) dfft::fail(dfft::kErrInvalidArgument, "null descriptor");
+  if (d->rank < 2 || d->rank > DFFT_MAX_RANK) dfft::fail(dfft::kErrInvalidArgument, "view rank must be in [2, 4]");
+  if (d->fft_rank < 1 || d->fft_rank > 3 || d->fft_rank > d->rank)
+    dfft::fail(dfft::kErrInvalidArgument, "the Rank of FFT axes must be between 1 and 3");
+  dfft::PlanDesc p;
+  const std::size_t D = static_cast<std::size_t>(d->rank);
+  for (int i = 0; i < d->fft_rank; ++i) {
+    int a = d->axes[i];
+    if (a < 0) a += d->rank;  // convert_negative_axes
+    if (a < 0 || a >= d->rank) dfft::fail(dfft::kErrInvalidArgument, "input axes are not valid for the view");
+    p.axes.push_back(static_cast<std::size_t>(a));
+  }
+  for (std::size_t k = 0; k < D; ++k) {
+    p.gin.push_back(d->in_extents[k]);
+    p.gout.push_back(d->out_extents[k]);
+    p.in_topo.push_back(d->in_topology[k]);
+    p.out_topo.push_back(d->out_topology[k]);
+  }
+  p.in_right = d->in_topology_layout_right != 0;
+  p.out_right = d->out_topology_layout_right != 0;
+  p.view_right = d->view_layout_right != 0;
+  if (d->kind != DFFT_KIND_C2C && d->kind != DFFT_KIND_R2C) dfft::fail(dfft::kErrInvalidArgument, "unknown kind");
+  if (d->precision != DFFT_PREC_F64 && d->precision != DFFT_PREC_F32)
+    dfft::fail(dfft::kErrInvalidArgument, "unknown precision");
+  if (d->exec_mode != DFFT_EXEC_FUSED && d->exec_mode != DFFT_EXEC_LITERAL)
+    dfft::fail(dfft::kErrInvalidArgument, "unknown execution mode");
+  p.r2c = d->kind == DFFT_KIND_R2C;
+  p.dbl = d->precision == DFFT_PREC_F64;
+  p.norm = d->normalization;
+  p.exec_mode = d->exec_mode;
+  p.stream = static_cast<cudaStream_t>(d->stream);
+  return p;
+}
+
+const dfft::Plan& impl_of(const dfft_plan* p) {
+  if (!p || !p->impl) dfft::fail(dfft::kErrInvalidArgument, "null plan");
+  return *p->impl;
+}
+
+void copy_ext(const dfft::Ext& e, uint64_t* dst, std::size_t n) {
+  for (std::size_t i = 0; i < n; ++i) dst[i] = i < e.size() ? e[i] : 0;
+}
+
+dfft_status create(dfft_plan** out, const dfft_plan_desc* desc, bool on_device) {
+  return guarded([&] {
+    if (!out) dfft::fail(dfft::kErrInvalidArgument, "null output pointer");
+    *out = nullptr;
+    auto p = to_desc(desc);
+    auto* impl = new dfft::Plan(p, on_device);
+    *out = new dfft_plan_s{impl};
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+void dfft_plan_desc_init(dfft_plan_desc* d) {
+  if (!d) return;
+  std::memset(d, 0, sizeof(*d));
+  d->rank = 3;
+  d->fft_rank = 3;
+  d->axes[0] = 0;
+  d->axes[1] = 1;
+  d->axes[2] = 2;
+  for (int k = 0; k < DFFT_MAX_RANK; ++k) {
+    d->in_topology[k] = 1;
+    d->out_topology[k] = 1;
+  }
+  d->in_topology_layout_right = 1;
+  d->out_topology_layout_right = 1;
+  d->view_layout_right = 1;
+  d->kind = DFFT_KIND_C2C;
+  d->precision = DFFT_PREC_F64;
+  d->normalization = DFFT_NORM_BACKWARD;
+  d->exec_mode = DFFT_EXEC_FUSED;
+  d->stream = nullptr;
+}
+
+dfft_status dfft_plan_create(dfft_plan** plan, const dfft_plan_desc* desc) { return create(plan, desc, true); }
+
+dfft_status dfft_plan_analyze(dfft_plan** plan, const dfft_plan_desc* desc) { return create(plan, desc, false); }
+
+dfft_status dfft_plan_destroy(dfft_plan* plan) {
+  return guarded([&] {
+    if (!plan) return;
+    delete plan->impl;
+    delete plan;
+  });
+}
+
+dfft_status dfft_execute_on_stream(const dfft_plan* plan, const void* in, void* out, int32_t direction,
+                                   void* stream) {
+  return guarded([&] {
+    const auto& p = impl_of(plan);
+    if (direction != DFFT_FORWARD && direction != DFFT_BACKWARD)
+      dfft::fail(dfft::kErrInvalidArgument, "Invalid FFT direction specified.");
+    p.execute(in, out, direction == DFFT_FORWARD, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_execute(const dfft_plan* plan, const void* in, void* out, int32_t direction) {
+  if (!plan || !plan->impl) return set_error(DFFT_ERROR_INVALID_ARGUMENT, "null plan");
+  return dfft_execute_on_stream(plan, in, out, direction, plan->impl->desc().stream);
+}
+
+const char* dfft_plan_name(const dfft_plan* plan) {
+  if (!plan || !plan->impl) return "";
+  return plan->impl->name().c_str();
+}
+
+dfft_status dfft_get_nprocs(const dfft_plan* plan, int64_t* nprocs) {
+  return guarded([&] {
+    if (!nprocs) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *nprocs = static_cast<int64_t>(impl_of(plan).nprocs());
+  });
+}
+
+dfft_status dfft_get_local_extents(const dfft_plan* plan, int64_t rank, int32_t which, uint64_t* extents,
+                                   uint64_t* starts) {
+  return guarded([&] {
+    const auto& p = impl_of(plan);
+    if (rank < 0 || static_cast<std::size_t>(rank) >= p.nprocs())
+      dfft::fail(dfft::kErrInvalidArgument, "rank must be less than topology size.");
+    const dfft::Layout& L = which == 0 ? p.in_layout() : p.out_layout();
+    const std::size_t D = L.gext.size();
+    dfft::Ext ext = dfft::compute_local_extents(L.gext, L.topo, dfft::identity_map(D), rank, L.rank_right);
+    dfft::Ext st = dfft::compute_local_starts(L.gext, L.topo, rank, L.rank_right);
+    if (extents) copy_ext(ext, extents, DFFT_MAX_RANK);
+    if (starts) copy_ext(st, starts, DFFT_MAX_RANK);
+  });
+}
+
+dfft_status dfft_get_local_offset(const dfft_plan* plan, int64_t rank, int32_t which, uint64_t* offset) {
+  return guarded([&] {
+    const auto& p = impl_of(plan);
+    if (rank < 0 || static_cast<std::size_t>(rank) >= p.nprocs())
+      dfft::fail(dfft::kErrInvalidArgument, "rank must be less than topology size.");
+    if (!offset) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    auto blocks = dfft::layout_blocks(which == 0 ? p.in_layout() : p.out_layout());
+    *offset = blocks[rank].base;
+  });
+}
+
+dfft_status dfft_get_buffer_elements(const dfft_plan* plan, int32_t which, uint64_t* count) {
+  return guarded([&] {
+    const auto& p = impl_of(plan);
+    if (!count) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *count = dfft::layout_elements(which == 0 ? p.in_layout() : p.out_layout());
+  });
+}
+
+dfft_status dfft_get_num_blocks(const dfft_plan* plan, int64_t* nblocks) {
+  return guarded([&] {
+    if (!nblocks) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *nblocks = static_cast<int64_t>(impl_of(plan).analyses().at(0).blocks.size());
+  });
+}
+
+dfft_status dfft_get_block_info(const dfft_plan* plan, int64_t rank, int64_t block, dfft_block_info* info) {
+  return guarded([&] {
+    const auto& p = impl_of(plan);
+    if (!info) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    if (rank < 0 || static_cast<std::size_t>(rank) >= p.nprocs())
+      dfft::fail(dfft::kErrInvalidArgument, "rank must be less than topology size.");
+    const auto& blocks = p.analyses().at(rank).blocks;
+    if (block < 0 || static_cast<std::size_t>(block) >= blocks.size())
+      dfft::fail(dfft::kErrInvalidArgument, "block index out of range");
+    const auto& b = blocks[block];
+    std::memset(info, 0, sizeof(*info));
+    info->block_type = b.block_type == dfft::BlockType::FFT ? 1 : 0;
+    info->block_idx = static_cast<int32_t>(b.block_idx);
+    info->fft_dim = static_cast<int32_t>(b.fft_dim);
+    info->in_axis = static_cast<int32_t>(b.in_axis);
+    info->out_axis = static_cast<int32_t>(b.out_axis);
+    info->comm_axis = static_cast<int32_t>(b.comm_axis);
+    copy_ext(b.in_topology, info->in_topology, DFFT_MAX_RANK);
+    copy_ext(b.out_topology, info->out_topology, DFFT_MAX_RANK);
+    copy_ext(b.in_extents, info->in_extents, DFFT_MAX_RANK);
+    copy_ext(b.out_extents, info->out_extents, DFFT_MAX_RANK);
+    copy_ext(b.buffer_extents, info->buffer_extents, DFFT_MAX_RANK + 1);
+    copy_ext(b.in_map, info->in_map, DFFT_MAX_RANK);
+    copy_ext(b.out_map, info->out_map, DFFT_MAX_RANK);
+  });
+}
+
+dfft_status dfft_get_max_buffer_size(const dfft_plan* plan, uint64_t* size) {
+  return guarded([&] {
+    if (!size) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *size = impl_of(plan).max_buffer_size();
+  });
+}
+
+dfft_status dfft_get_topology_chain(const dfft_plan* plan, int64_t* n, uint64_t* topologies, int64_t* trans_axes,
+                                    int64_t* layouts) {
+  return guarded([&] {
+    const auto& p = impl_of(plan);
+    if (!n) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    const auto& ch = p.chain();
+    const int64_t cap = *n;
+    *n = static_cast<int64_t>(ch.size());
+    if (cap < static_cast<int64_t>(ch.size())) return;
+    const std::size_t D = p.desc().gin.size();
+    for (std::size_t i = 0; i < ch.size(); ++i) {
+      if (topologies)
+        for (std::size_t k = 0; k < D; ++k) topologies[i * D + k] = ch[i][k];
+      if (layouts) layouts[i] = static_cast<int64_t>(p.chain_layouts().at(i));
+      if (trans_axes && i + 1 < ch.size())
+        trans_axes[i] = i < p.chain_trans_axes().size() ? static_cast<int64_t>(p.chain_trans_axes()[i]) : 0;
+    }
+  });
+}
+
+dfft_status dfft_debug_export_buffers(const dfft_plan* plan, int32_t direction, int64_t block, int32_t which,
+                                      void* host_dst, uint64_t capacity_bytes) {
+  return guarded([&] {
+    if (!host_dst) dfft::fail(dfft::kErrInvalidArgument, "null host buffer");
+    if (block < 0) dfft::fail(dfft::kErrInvalidArgument, "block index out of range");
+    impl_of(plan).export_buffers(direction == DFFT_FORWARD, static_cast<std::size_t>(block), which, host_dst,
+                                 capacity_bytes);
+  });
+}
+
+dfft_status dfft_get_launch_count(const dfft_plan* plan, int32_t direction, int64_t* launches) {
+  return guarded([&] {
+    if (!launches) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *launches = static_cast<int64_t>(impl_of(plan).launches(direction == DFFT_FORWARD));
+  });
+}
+
+dfft_status dfft_get_workspace_bytes(const dfft_plan* plan, uint64_t* bytes) {
+  return guarded([&] {
+    if (!bytes) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *bytes = impl_of(plan).workspace_bytes();
+  });
+}
+
+const char* dfft_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* dfft_version(void) { return "dfft-b200 0.1.0"; }
+
+}  // extern "C"

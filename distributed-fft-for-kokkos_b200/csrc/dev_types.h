@@ -1,0 +1,70 @@
+// Host-visible argument structs and launchers of the device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace dfft {
+namespace dev {
+
+// Layout lookup tables (see layout.hpp).  Offsets index into `t`.
+struct DevLayout {
+  const int64_t* t;
+  int mode;  // 0 separable, 1 general
+  int64_t off[4], rk[4], loc[4], rbase, rstride;
+};
+
+enum StageKind { kC2C = 0, kR2C = 1, kC2R = 2, kCopy = 3 };
+
+constexpr int kMaxPasses = 16;
+
+struct StageArgs {
+  DevLayout src, dst;
+  const void* in;
+  void* out;
+  const void* tw;     // n twiddles exp(-2*pi*i*k/n) in the stage precision
+  int nd;             // view rank
+  int a, b, o0, o1;   // FFT axis, tile axis, remaining axes (-1 if absent)
+  int n;              // transform length (real length for R2C / C2R)
+  int na_in, na_out;  // extents along a in the source / destination
+  int Eb, Eo0, Eo1;   // extents along b, o0, o1
+  int B;              // lines per tile (real lines for R2C / C2R)
+  int nl;             // shared-memory lines (B, or ceil(B/2) for R2C / C2R)
+  int pitch;          // shared-memory line pitch (complex elements)
+  int tiles_b;        // ceil(Eb / B)
+  int load_afast, store_afast;  // thread order of the gather / scatter
+  double scale;                 // applied on store
+  int npass;
+  unsigned long long radix_code;  // radix of pass p in bits [4p, 4p+4)
+};
+
+// Per-rank geometry of one transpose, packed as int64:
+//   [r*rs + 0..3]   starts of rank r's block (logical axes)
+//   [r*rs + 4..7]   extents of rank r's block (logical axes)
+//   [r*rs + 8]      sub-rank of r in its exchange group
+//   [r*rs + 9..]    world ranks of the group members, by sub-rank (pc entries)
+struct XposeArgs {
+  const int64_t* geo;
+  int rs;           // int64 per rank in geo
+  int nd;           // view rank
+  int nprocs;       // world size P
+  int pc;           // exchange group size (buffer extent of the rank dim)
+  int axis;         // pack: split axis; unpack: merged axis
+  int64_t merged;   // global extent along `axis`
+  int64_t bext[5];  // buffer extents (reference order)
+  int buf_right;    // buffer memory order: rank dim first (LayoutRight) or last
+  int64_t bufsize;  // elements per rank buffer
+  DevLayout lay;    // global array layout (pack source / unpack destination)
+  const void* src;
+  void* dst;
+};
+
+cudaError_t launch_fft_stage(const StageArgs& A, bool dbl, int kind, bool inverse, int nthreads, size_t smem,
+                             unsigned tiles, cudaStream_t st);
+// op: 0 pack, 1 all-to-all, 2 unpack
+cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
+cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);
+
+}  // namespace dev
+}  // namespace dfft

@@ -1,0 +1,706 @@
+// Plan construction and execution.
+//
+// Validation follows internal_plan_factory (KokkosFFT_Distributed_Plan.hpp:46-113)
+// and the Slab/Pencil plan constructors; the block lists come from the
+// restated block analyses; normalisation follows the SlabPlan / PencilPlan
+// wrappers (KokkosFFT_Distributed_SlabPlan.hpp:1344-1358,
+// KokkosFFT_Distributed_PencilPlan.hpp:1680-1690).
+//
+// Two device programs exist per direction:
+//   fused   - one FFT stage kernel per FFT axis.  The first stage gathers from
+//             the caller's input blocks, the last scatters into the caller's
+//             output blocks, the stages in between use a plain global array.
+//             Every exchange of the reference (pack, all-to-all, unpack, local
+//             transposes) is a re-addressing inside those gathers / scatters,
+//             and the normalisation is a factor in the last scatter.
+//   literal - the reference's block sequence kernel by kernel on per-rank
+//             blocks: local transpose, per-axis FFTs, pack, all-to-all,
+//             unpack, normalisation pass.  Its send / recv buffers are kept
+//             for bit-exact comparison with the reference's buffers.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace dfft {
+
+namespace {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) fail(kErrCuda, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Radix plan of a transform length: passes of 8 (with 4,4 or 4 or 2 to finish
+// a power of two), then 3, 5, 7, 11, 13.
+std::vector<int> radix_plan(std::size_t n) {
+  std::vector<int> r;
+  std::size_t m = n;
+  int k2 = 0;
+  while (m % 2 == 0) {
+    m /= 2;
+    ++k2;
+  }
+  int q = k2 / 3, rem = k2 % 3;
+  if (rem == 1) {
+    if (q >= 1) {
+      --q;
+      r.push_back(4);
+      r.push_back(4);
+    } else {
+      r.push_back(2);
+    }
+  } else if (rem == 2) {
+    r.push_back(4);
+  }
+  for (int i = 0; i < q; ++i) r.push_back(8);
+  for (int p : {3, 5, 7, 11, 13}) {
+    while (m % static_cast<std::size_t>(p) == 0) {
+      m /= static_cast<std::size_t>(p);
+      r.push_back(p);
+    }
+  }
+  if (m != 1)
+    fail(kErrUnsupported, "FFT length " + std::to_string(n) + " has a prime factor larger than 13");
+  if (r.size() > static_cast<std::size_t>(dev::kMaxPasses)) fail(kErrUnsupported, "too many FFT passes");
+  return r;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Construction
+// ---------------------------------------------------------------------------
+Plan::Plan(const PlanDesc& d, bool on_device) : d_(d), on_device_(on_device) {
+  analyze();
+  if (!on_device_) return;
+  try {
+    build_fused(true);
+    build_fused(false);
+    if (d_.exec_mode == 1) {
+      prog_[0].clear();
+      prog_[1].clear();
+      build_literal(true);
+      build_literal(false);
+    }
+    allocate_device();
+  } catch (...) {
+    for (auto p : bufs_)
+      if (p) cudaFree(p);
+    for (auto& kv : twiddles_) cudaFree(kv.second);
+    if (d_tables_) cudaFree(d_tables_);
+    throw;
+  }
+}
+
+Plan::~Plan() {
+  for (auto p : bufs_)
+    if (p) cudaFree(p);
+  for (auto& kv : twiddles_) cudaFree(kv.second);
+  if (d_tables_) cudaFree(d_tables_);
+}
+
+void Plan::analyze() {
+  const std::size_t D = d_.gin.size();
+  if (D < 2 || D > static_cast<std::size_t>(kMaxRank)) fail(kErrInvalidArgument, "view rank must be in [2, 4]");
+  if (d_.gout.size() != D || d_.in_topo.size() != D || d_.out_topo.size() != D)
+    fail(kErrInvalidArgument, "extents and topologies must have the view rank");
+  for (std::size_t k = 0; k < D; ++k) {
+    if (d_.gin[k] == 0 || d_.gout[k] == 0) fail(kErrInvalidExtents, "extents must be positive");
+    if (d_.gin[k] >= (1u << 30) || d_.gout[k] >= (1u << 30)) fail(kErrUnsupported, "extent too large");
+  }
+  // internal_plan_factory (Plan.hpp:59-72)
+  if (total_size(d_.in_topo) != total_size(d_.out_topo))
+    fail(kErrInvalidTopology, "in_topology and out_topology must have the same size.");
+  check_valid_extents(d_.gin, d_.gout, d_.axes, d_.r2c, d_.view_right);
+
+  type_ = get_common_topology_type({d_.in_topo, d_.out_topo});
+  switch (type_) {
+    case TopologyType::Shared: name_ = "SharedPlan"; break;
+    case TopologyType::Slab: name_ = "SlabPlan"; break;
+    case TopologyType::Pencil:
+      if (D < 3) fail(kErrInvalidTopology, "Pencil plan supports 3D or higher dimensional Views");
+      name_ = "PencilPlan";
+      break;
+    case TopologyType::Empty: fail(kErrInvalidTopology, "Empty topology is not supported for FFT plan.");
+    case TopologyType::Brick: fail(kErrInvalidTopology, "Brick topology is not supported for FFT plan.");
+    default: fail(kErrInvalidTopology, "Unsupported topology for FFT plan.");
+  }
+
+  const std::size_t P = nprocs();
+  if (type_ == TopologyType::Slab) {
+    chain_ = get_all_slab_topologies(d_.in_topo, d_.out_topo, d_.axes);
+    chain_layouts_.assign(chain_.size(), 1);
+    trans_axes_.assign(chain_.size() - 1, 0);
+  } else if (type_ == TopologyType::Pencil) {
+    auto ch = get_all_pencil_topologies(d_.in_topo, d_.in_right, d_.out_topo, d_.out_right, d_.axes);
+    chain_ = ch.topologies;
+    trans_axes_ = ch.trans_axes;
+    chain_layouts_ = ch.layouts;
+  } else {
+    chain_ = {d_.in_topo};
+    chain_layouts_ = {d_.in_right ? 1u : 0u};
+  }
+
+  per_rank_.resize(P);
+  for (std::size_t r = 0; r < P; ++r) {
+    Ext in_ext = compute_local_extents(d_.gin, d_.in_topo, identity_map(D), r, d_.in_right);
+    if (type_ == TopologyType::Slab) {
+      per_rank_[r] = slab_block_analyses(in_ext, d_.gin, d_.gout, d_.in_topo, d_.out_topo, d_.axes, d_.r2c,
+                                         d_.view_right, r);
+      if (per_rank_[r].blocks.empty() || per_rank_[r].blocks.size() > 5)
+        fail(kErrInternal, "Number blocks must be in [1, 5]");
+    } else if (type_ == TopologyType::Pencil) {
+      per_rank_[r] = pencil_block_analyses(in_ext, d_.gin, d_.gout, d_.in_topo, d_.in_right, d_.out_topo,
+                                           d_.out_right, d_.axes, d_.r2c, d_.view_right, r);
+      if (per_rank_[r].blocks.empty() || per_rank_[r].blocks.size() > 8)
+        fail(kErrInternal, "Number blocks must be in [1, 8]");
+    } else {
+      // SharedPlan (KokkosFFT_Distributed_SharedPlan.hpp:15-84): one local FFT.
+      BlockInfo b;
+      Ext map = get_map_axes(D, d_.axes, d_.view_right);
+      b.block_type = BlockType::FFT;
+      b.fft_dim = d_.axes.size();
+      b.in_map = b.out_map = map;
+      b.in_extents = compute_mapped_extents(d_.gin, map);
+      b.out_extents = compute_mapped_extents(d_.gout, map);
+      b.in_topology.assign(D, 0);
+      b.out_topology.assign(D, 0);
+      b.buffer_extents.assign(D + 1, 0);
+      per_rank_[r].blocks = {b};
+      per_rank_[r].max_buffer_size = total_size(d_.gout) * 2;
+    }
+    max_buffer_size_ = std::max(max_buffer_size_, per_rank_[r].max_buffer_size);
+  }
+
+  // Normalisation (KokkosFFT::Impl::normalize semantics).
+  Ext fft_ext = compute_fft_extents(d_.gin, d_.gout, d_.axes);
+  const double N = static_cast<double>(total_size(fft_ext));
+  switch (d_.norm) {
+    case 0: scale_fwd_ = 1.0; scale_bwd_ = 1.0 / N; break;
+    case 1: scale_fwd_ = 1.0 / N; scale_bwd_ = 1.0; break;
+    case 2: scale_fwd_ = scale_bwd_ = 1.0 / std::sqrt(N); break;
+    case 3: scale_fwd_ = scale_bwd_ = 1.0; break;
+    default: fail(kErrInvalidArgument, "unknown normalization");
+  }
+
+  lin_.gext = d_.gin;
+  lin_.topo = d_.in_topo;
+  lin_.rank_right = d_.in_right;
+  lin_.map = identity_map(D);
+  lin_.view_right = d_.view_right;
+  lin_.complex = !d_.r2c;
+  lout_.gext = d_.gout;
+  lout_.topo = d_.out_topo;
+  lout_.rank_right = d_.out_right;
+  lout_.map = identity_map(D);
+  lout_.view_right = d_.view_right;
+  lout_.complex = true;
+}
+
+int Plan::add_layout(const Layout& L) {
+  for (std::size_t i = 0; i < layouts_.size(); ++i)
+    if (layouts_[i] == L) return static_cast<int>(i);
+  layouts_.push_back(L);
+  tables_.push_back(build_layout_tables(L));
+  layout_base_.push_back(static_cast<std::int64_t>(host_tables_.size()));
+  auto& t = tables_.back().data;
+  host_tables_.insert(host_tables_.end(), t.begin(), t.end());
+  return static_cast<int>(layouts_.size() - 1);
+}
+
+Layout Plan::block_layout(const Ext& topo, bool rank_right, const Ext& map, bool complex) const {
+  Layout L;
+  L.gext = complex ? d_.gout : d_.gin;
+  L.topo = topo;
+  L.rank_right = rank_right;
+  L.map = map;
+  L.view_right = d_.view_right;
+  L.complex = complex;
+  return L;
+}
+
+// FFT axes in the order the reference transforms them in the forward
+// direction: FFT blocks in sequence, each block's axes from the innermost
+// (unit-stride) one outwards.  The first axis is the R2C axis.
+std::vector<std::size_t> Plan::fft_axis_order() const {
+  std::vector<std::size_t> order;
+  const std::size_t D = d_.gin.size();
+  for (auto& b : per_rank_.at(0).blocks) {
+    if (b.block_type != BlockType::FFT) continue;
+    for (std::size_t i = 0; i < b.fft_dim; ++i) order.push_back(d_.view_right ? b.in_map[D - 1 - i] : b.in_map[i]);
+  }
+  Ext sorted_order(order.begin(), order.end()), sorted_axes = d_.axes;
+  std::sort(sorted_order.begin(), sorted_order.end());
+  std::sort(sorted_axes.begin(), sorted_axes.end());
+  if (sorted_order != sorted_axes) fail(kErrInternal, "FFT blocks do not cover the FFT axes");
+  return order;
+}
+
+const void* Plan::twiddle(std::size_t n) {
+  auto key = std::make_pair(n, d_.dbl);
+  auto it = twiddles_.find(key);
+  if (it != twiddles_.end()) return it->second;
+  const long double pi = 3.141592653589793238462643383279502884L;
+  std::vector<double> hd(2 * n);
+  std::vector<float> hf(2 * n);
+  for (std::size_t k = 0; k < n; ++k) {
+    const long double ang = 2.0L * pi * static_cast<long double>(k) / static_cast<long double>(n);
+    const long double c = cosl(ang), s = -sinl(ang);
+    hd[2 * k] = static_cast<double>(c);
+    hd[2 * k + 1] = static_cast<double>(s);
+    hf[2 * k] = static_cast<float>(c);
+    hf[2 * k + 1] = static_cast<float>(s);
+  }
+  void* p = nullptr;
+  const std::size_t bytes = n * (d_.dbl ? 16 : 8);
+  if (cudaMalloc(&p, bytes) != cudaSuccess) fail(kErrAlloc, "cudaMalloc of twiddle table failed");
+  twiddles_[key] = p;
+  workspace_bytes_ += bytes;
+  cuda_check(cudaMemcpy(p, d_.dbl ? static_cast<const void*>(hd.data()) : static_cast<const void*>(hf.data()), bytes,
+                        cudaMemcpyHostToDevice),
+             "twiddle upload");
+  return p;
+}
+
+Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse, double scale) {
+  const Layout& S = layouts_[src_l];
+  const Layout& Dl = layouts_[dst_l];
+  const std::size_t D = S.gext.size();
+  Op op;
+  op.type = Op::Stage;
+  op.kind = kind;
+  op.inverse = inverse;
+  op.src_layout = src_l;
+  op.dst_layout = dst_l;
+  dev::StageArgs& A = op.sa;
+  std::memset(&A, 0, sizeof(A));
+  const std::size_t n = (kind == dev::kC2R) ? Dl.gext[a] : S.gext[a];
+  A.nd = static_cast<int>(D);
+  A.a = static_cast<int>(a);
+  A.n = static_cast<int>(n);
+  A.na_in = static_cast<int>(S.gext[a]);
+  A.na_out = static_cast<int>(Dl.gext[a]);
+  if (kind == dev::kCopy && A.na_in != A.na_out) fail(kErrInternal, "copy stage with different extents");
+  const std::size_t fs = layout_fast_axis(S), fd = layout_fast_axis(Dl);
+  std::size_t b;
+  if (fd != a) b = fd;
+  else if (fs != a) b = fs;
+  else b = (a == 0) ? 1 : 0;
+  A.b = static_cast<int>(b);
+  int others[2] = {-1, -1}, no = 0;
+  for (std::size_t k = 0; k < D; ++k)
+    if (k != a && k != b) others[no++] = static_cast<int>(k);
+  A.o0 = others[0];
+  A.o1 = others[1];
+  A.Eb = static_cast<int>(Dl.gext[b]);
+  A.Eo0 = A.o0 >= 0 ? static_cast<int>(Dl.gext[A.o0]) : 1;
+  A.Eo1 = A.o1 >= 0 ? static_cast<int>(Dl.gext[A.o1]) : 1;
+  A.load_afast = fs == a ? 1 : 0;
+  A.store_afast = fd == a ? 1 : 0;
+  A.scale = scale;
+
+  if (kind != dev::kCopy) {
+    auto radices = radix_plan(n);
+    A.npass = static_cast<int>(radices.size());
+    unsigned long long code = 0;
+    for (std::size_t p = 0; p < radices.size(); ++p) code |= static_cast<unsigned long long>(radices[p]) << (4 * p);
+    A.radix_code = code;
+  }
+
+  const std::size_t ce = d_.dbl ? 16 : 8;
+  const bool pairs = kind == dev::kR2C || kind == dev::kC2R;
+  const std::size_t base = kind == dev::kC2R ? 2 * (n / 2 + 1) : n;
+  const std::size_t pitch = base | 1;
+  auto smem_for = [&](std::size_t B) {
+    const std::size_t nl = pairs ? (B + 1) / 2 : B;
+    return ((n + 1) & ~static_cast<std::size_t>(1)) * ce + 2 * nl * pitch * ce;
+  };
+  std::size_t B = std::min<std::size_t>(d_.dbl ? 8 : 16, Dl.gext[b]);
+  if (pairs && B > 1 && (B & 1)) ++B;
+  while (B > 1 && smem_for(B) > 100 * 1024) B = pairs ? std::max<std::size_t>(2, B - 2) : B - 1;
+  if (B == 2 && pairs && smem_for(B) > 100 * 1024) B = 2;
+  if (smem_for(B) > 227 * 1024) fail(kErrUnsupported, "FFT length " + std::to_string(n) + " too large for one stage");
+  A.B = static_cast<int>(B);
+  A.nl = static_cast<int>(pairs ? (B + 1) / 2 : B);
+  A.pitch = static_cast<int>(pitch);
+  A.tiles_b = static_cast<int>((Dl.gext[b] + B - 1) / B);
+  const unsigned long long tiles = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
+  if (tiles >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
+  op.tiles = static_cast<unsigned>(tiles);
+  op.smem = smem_for(B);
+  op.nthreads = 256;
+  if (kind != dev::kCopy) A.tw = twiddle(n);
+  return op;
+}
+
+// ---------------------------------------------------------------------------
+// Fused program
+// ---------------------------------------------------------------------------
+void Plan::build_fused(bool forward) {
+  auto& prog = prog_[forward ? 0 : 1];
+  prog.clear();
+  auto order = fft_axis_order();
+  const std::size_t S = order.size();
+  Layout I;
+  I.gext = d_.gout;
+  I.topo.assign(d_.gout.size(), 1);
+  I.map = identity_map(d_.gout.size());
+  I.view_right = d_.view_right;
+  I.complex = true;
+  const int li = add_layout(I), lin = add_layout(lin_), lout = add_layout(lout_);
+  if (!forward) std::reverse(order.begin(), order.end());
+  for (std::size_t s = 0; s < S; ++s) {
+    const bool first = s == 0, last = s == S - 1;
+    int src_l, dst_l, kind;
+    if (forward) {
+      src_l = first ? lin : li;
+      dst_l = last ? lout : li;
+      kind = (first && d_.r2c) ? dev::kR2C : dev::kC2C;
+    } else {
+      src_l = first ? lout : li;
+      dst_l = last ? lin : li;
+      kind = (last && d_.r2c) ? dev::kC2R : dev::kC2C;
+    }
+    Op op = make_stage(src_l, dst_l, order[s], kind, !forward, last ? (forward ? scale_fwd_ : scale_bwd_) : 1.0);
+    op.src = first ? kBufIn : (((s - 1) % 2 == 0) ? kBufScratch0 : kBufScratch1);
+    op.dst = last ? kBufOut : ((s % 2 == 0) ? kBufScratch0 : kBufScratch1);
+    prog.push_back(op);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Literal program (reference block sequence)
+// ---------------------------------------------------------------------------
+std::int64_t Plan::add_geo(const Layout& L, const BlockInfo& b, std::size_t pc) {
+  const std::size_t P = nprocs();
+  auto blocks = layout_blocks(L);
+  // Exchange groups: the whole communicator for slabs; for pencils the row /
+  // column communicators of MPI_Cart_create over the non-one entries of the
+  // input topology (reorder = 0, row-major) split by MPI_Cart_sub
+  // (KokkosFFT_Distributed_PencilPlan.hpp:32-71), picked by comm_axis.
+  std::vector<std::size_t> dims;
+  for (auto t : d_.in_topo)
+    if (t > 1) dims.push_back(t);
+  const std::int64_t base = static_cast<std::int64_t>(host_tables_.size());
+  for (std::size_t r = 0; r < P; ++r) {
+    for (int k = 0; k < 4; ++k)
+      host_tables_.push_back(k < static_cast<int>(L.gext.size()) ? static_cast<std::int64_t>(blocks[r].starts[k]) : 0);
+    for (int k = 0; k < 4; ++k)
+      host_tables_.push_back(k < static_cast<int>(L.gext.size()) ? static_cast<std::int64_t>(blocks[r].local[k]) : 0);
+    std::size_t sub = r;
+    std::vector<std::size_t> members(pc);
+    if (type_ == TopologyType::Pencil) {
+      const std::size_t t1 = dims.at(1);
+      const std::size_t c0 = r / t1, c1 = r % t1;
+      if (b.comm_axis == 0) {
+        if (pc != dims.at(0)) fail(kErrInternal, "row communicator size mismatch");
+        sub = c0;
+        for (std::size_t j = 0; j < pc; ++j) members[j] = j * t1 + c1;
+      } else {
+        if (pc != t1) fail(kErrInternal, "column communicator size mismatch");
+        sub = c1;
+        for (std::size_t j = 0; j < pc; ++j) members[j] = c0 * t1 + j;
+      }
+    } else {
+      if (pc != P) fail(kErrInternal, "communicator size mismatch");
+      for (std::size_t j = 0; j < pc; ++j) members[j] = j;
+    }
+    host_tables_.push_back(static_cast<std::int64_t>(sub));
+    for (auto m : members) host_tables_.push_back(static_cast<std::int64_t>(m));
+  }
+  return base;
+}
+
+void Plan::build_literal(bool forward) {
+  auto& prog = prog_[forward ? 0 : 1];
+  prog.clear();
+  const auto& blocks = per_rank_.at(0).blocks;
+  const std::size_t D = d_.gin.size();
+  const std::size_t nbl = blocks.size();
+  std::vector<std::size_t> topo_index(nbl);  // chain index of each block
+  {
+    std::size_t t = 0;
+    for (std::size_t i = 0; i < nbl; ++i) {
+      topo_index[i] = t;
+      if (blocks[i].block_type == BlockType::Transpose) ++t;
+    }
+  }
+  auto flag = [&](std::size_t k) { return chain_layouts_.at(k) != 0; };
+  auto other_scratch = [](int b) { return b == kBufScratch0 ? kBufScratch1 : kBufScratch0; };
+  auto copy_to = [&](int& cur_l, int& cur_b, const Layout& L) {
+    const int nl = add_layout(L);
+    if (nl == cur_l) return;
+    // a local transpose: lines along the source's unit-stride axis
+    Op op = make_stage(cur_l, nl, layout_fast_axis(layouts_[cur_l]), dev::kCopy, false, 1.0);
+    op.src = cur_b;
+    op.dst = other_scratch(cur_b);
+    prog.push_back(op);
+    cur_l = nl;
+    cur_b = op.dst;
+  };
+  auto fft_stage = [&](int& cur_l, int& cur_b, const Layout& dstL, std::size_t a, int kind, bool inv) {
+    const int nl = add_layout(dstL);
+    Op op = make_stage(cur_l, nl, a, kind, inv, 1.0);
+    op.src = cur_b;
+    // in place on scratch; out of place when reading the caller's buffer or changing type
+    op.dst = (cur_b == kBufIn || kind == dev::kR2C || kind == dev::kC2R) ? other_scratch(cur_b) : cur_b;
+    prog.push_back(op);
+    cur_l = nl;
+    cur_b = op.dst;
+  };
+  auto xpose = [&](int& cur_l, int& cur_b, const BlockInfo& b, const Layout& Ls, const Layout& Ld,
+                   std::size_t pack_axis, std::size_t unpack_axis, int dir) {
+    const int ls = add_layout(Ls), ld = add_layout(Ld);
+    if (ls != cur_l) copy_to(cur_l, cur_b, Ls);
+    const std::size_t pc = d_.view_right ? b.buffer_extents.front() : b.buffer_extents.back();
+    const std::size_t bufsize = total_size(b.buffer_extents);
+    const int eb = Ls.complex ? (d_.dbl ? 16 : 8) : (d_.dbl ? 8 : 4);
+    // debug send / recv buffers of this block and direction
+    std::size_t block_index = 0;
+    for (std::size_t i = 0; i < nbl; ++i)
+      if (&blocks[i] == &b) block_index = i;
+    int ids[2];
+    for (int w = 0; w < 2; ++w) {
+      ids[w] = static_cast<int>(kBufFirstDebug + debug_bufs_.size());
+      debug_bufs_[{dir, static_cast<int>(block_index * 2 + w)}] = ids[w];
+      buf_bytes_.resize(ids[w] + 1, 0);
+      buf_bytes_[ids[w]] = nprocs() * bufsize * eb;
+    }
+    dev::XposeArgs X;
+    std::memset(&X, 0, sizeof(X));
+    X.rs = static_cast<int>(9 + pc);
+    X.nd = static_cast<int>(D);
+    X.nprocs = static_cast<int>(nprocs());
+    X.pc = static_cast<int>(pc);
+    for (std::size_t k = 0; k < b.buffer_extents.size(); ++k) X.bext[k] = static_cast<std::int64_t>(b.buffer_extents[k]);
+    X.buf_right = d_.view_right ? 1 : 0;
+    X.bufsize = static_cast<std::int64_t>(bufsize);
+    Op pack;
+    pack.type = Op::Pack;
+    pack.xa = X;
+    pack.xa.axis = static_cast<int>(pack_axis);
+    pack.xa.merged = static_cast<std::int64_t>(Ls.gext[pack_axis]);
+    pack.src_layout = ls;
+    pack.xa.geo = reinterpret_cast<const std::int64_t*>(add_geo(Ls, b, pc));  // offset, resolved later
+    pack.elem_bytes = eb;
+    pack.src = cur_b;
+    pack.dst = ids[0];
+    pack.block = static_cast<int>(block_index);
+    Op a2a = pack;
+    a2a.type = Op::All2All;
+    a2a.src = ids[0];
+    a2a.dst = ids[1];
+    Op unpack;
+    unpack.type = Op::Unpack;
+    unpack.xa = X;
+    unpack.xa.axis = static_cast<int>(unpack_axis);
+    unpack.xa.merged = static_cast<std::int64_t>(Ld.gext[unpack_axis]);
+    unpack.dst_layout = ld;
+    unpack.xa.geo = reinterpret_cast<const std::int64_t*>(add_geo(Ld, b, pc));
+    unpack.elem_bytes = eb;
+    unpack.src = ids[1];
+    unpack.dst = other_scratch(cur_b);
+    unpack.block = static_cast<int>(block_index);
+    prog.push_back(pack);
+    prog.push_back(a2a);
+    prog.push_back(unpack);
+    cur_l = ld;
+    cur_b = unpack.dst;
+  };
+
+  const int dir = forward ? 0 : 1;
+  if (forward) {
+    int cur_l = add_layout(lin_), cur_b = kBufIn;
+    bool complex = lin_.complex;
+    for (std::size_t i = 0; i < nbl; ++i) {
+      const BlockInfo& b = blocks[i];
+      const std::size_t k = topo_index[i];
+      if (b.block_type == BlockType::FFT) {
+        Layout Lb = block_layout(chain_[k], flag(k), b.in_map, complex);
+        copy_to(cur_l, cur_b, Lb);
+        for (std::size_t j = 0; j < b.fft_dim; ++j) {
+          const std::size_t a = d_.view_right ? b.in_map[D - 1 - j] : b.in_map[j];
+          if (!complex) {
+            complex = true;
+            fft_stage(cur_l, cur_b, block_layout(chain_[k], flag(k), b.in_map, true), a, dev::kR2C, false);
+          } else {
+            fft_stage(cur_l, cur_b, layouts_[cur_l], a, dev::kC2C, false);
+          }
+        }
+      } else {
+        Layout Ls = block_layout(chain_[k], flag(k), b.in_map, complex);
+        Layout Ld = block_layout(chain_[k + 1], flag(k + 1), b.out_map, complex);
+        xpose(cur_l, cur_b, b, Ls, Ld, b.in_axis, b.out_axis, dir);
+      }
+    }
+    finalize_program(prog, cur_l, cur_b, lout_, scale_fwd_, true);
+  } else {
+    int cur_l = add_layout(lout_), cur_b = kBufIn;
+    bool complex = true;
+    for (std::size_t ii = nbl; ii-- > 0;) {
+      const BlockInfo& b = blocks[ii];
+      const std::size_t k = topo_index[ii];
+      if (b.block_type == BlockType::FFT) {
+        Layout Lb = block_layout(chain_[k], flag(k), b.in_map, true);
+        copy_to(cur_l, cur_b, Lb);
+        for (std::size_t jj = b.fft_dim; jj-- > 0;) {
+          const std::size_t a = d_.view_right ? b.in_map[D - 1 - jj] : b.in_map[jj];
+          const bool c2r = d_.r2c && b.block_idx == 0 && jj == 0;
+          if (c2r) {
+            complex = false;
+            fft_stage(cur_l, cur_b, block_layout(chain_[k], flag(k), b.in_map, false), a, dev::kC2R, true);
+          } else {
+            fft_stage(cur_l, cur_b, layouts_[cur_l], a, dev::kC2C, true);
+          }
+        }
+      } else {
+        Layout Ls = block_layout(chain_[k + 1], flag(k + 1), b.out_map, complex);
+        Layout Ld = block_layout(chain_[k], flag(k), b.in_map, complex);
+        xpose(cur_l, cur_b, b, Ls, Ld, b.out_axis, b.in_axis, dir);
+      }
+    }
+    finalize_program(prog, cur_l, cur_b, lin_, scale_bwd_, lin_.complex);
+  }
+}
+
+// Route the result of the program into the caller's output buffer (the last
+// op writes there directly when it already produces the output layout,
+// otherwise a local-transpose copy is appended), then normalise.
+void Plan::finalize_program(std::vector<Op>& prog, int cur_l, int cur_b, const Layout& final_layout, double scale,
+                            bool final_complex) {
+  const int lf = add_layout(final_layout);
+  if (cur_l == lf && !prog.empty() && prog.back().dst == cur_b && cur_b != kBufIn) {
+    prog.back().dst = kBufOut;
+  } else {
+    Op op = make_stage(cur_l, lf, layout_fast_axis(layouts_[cur_l]), dev::kCopy, false, 1.0);
+    op.src = cur_b;
+    op.dst = kBufOut;
+    prog.push_back(op);
+  }
+  if (scale != 1.0) {
+    Op s;
+    s.type = Op::Scale;
+    s.src = s.dst = kBufOut;
+    s.n_real = static_cast<std::int64_t>(layout_elements(final_layout) * (final_complex ? 2 : 1));
+    s.scale = scale;
+    prog.push_back(s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Device resources
+// ---------------------------------------------------------------------------
+void Plan::allocate_device() {
+  // Scratch: the largest global array the programs hold.
+  std::size_t max_elems = std::max(layout_elements(lin_), layout_elements(lout_));
+  const std::size_t scratch_bytes = max_elems * (d_.dbl ? 16 : 8);
+  buf_bytes_.resize(std::max<std::size_t>(buf_bytes_.size(), kBufFirstDebug), 0);
+  buf_bytes_[kBufScratch0] = scratch_bytes;
+  buf_bytes_[kBufScratch1] = scratch_bytes;
+  bufs_.assign(buf_bytes_.size(), nullptr);
+  // only allocate the scratch buffers the programs use
+  std::vector<bool> used(buf_bytes_.size(), false);
+  for (auto& prog : prog_)
+    for (auto& op : prog) {
+      if (op.src >= kBufScratch0) used[op.src] = true;
+      if (op.dst >= kBufScratch0) used[op.dst] = true;
+    }
+  for (std::size_t i = kBufScratch0; i < buf_bytes_.size(); ++i) {
+    if (!used[i] || buf_bytes_[i] == 0) continue;
+    if (cudaMalloc(&bufs_[i], buf_bytes_[i]) != cudaSuccess) {
+      cudaGetLastError();
+      fail(kErrAlloc, "cudaMalloc of " + std::to_string(buf_bytes_[i]) + " bytes of plan scratch failed");
+    }
+    workspace_bytes_ += buf_bytes_[i];
+  }
+  const std::size_t tb = std::max<std::size_t>(host_tables_.size(), 1) * sizeof(std::int64_t);
+  if (cudaMalloc(&d_tables_, tb) != cudaSuccess) {
+    cudaGetLastError();
+    fail(kErrAlloc, "cudaMalloc of layout tables failed");
+  }
+  workspace_bytes_ += tb;
+  if (!host_tables_.empty())
+    cuda_check(cudaMemcpy(d_tables_, host_tables_.data(), host_tables_.size() * sizeof(std::int64_t),
+                          cudaMemcpyHostToDevice),
+               "table upload");
+  auto dev_layout = [&](int l) {
+    dev::DevLayout L;
+    std::memset(&L, 0, sizeof(L));
+    const LayoutTables& T = tables_.at(l);
+    L.t = d_tables_ + layout_base_.at(l);
+    L.mode = T.mode;
+    for (int k = 0; k < 4; ++k) {
+      L.off[k] = T.off[k];
+      L.rk[k] = T.rk[k];
+      L.loc[k] = T.loc[k];
+    }
+    L.rbase = T.rbase;
+    L.rstride = T.rstride;
+    return L;
+  };
+  for (auto& prog : prog_) {
+    for (auto& op : prog) {
+      if (op.type == Op::Stage) {
+        op.sa.src = dev_layout(op.src_layout);
+        op.sa.dst = dev_layout(op.dst_layout);
+      } else if (op.type == Op::Pack || op.type == Op::All2All || op.type == Op::Unpack) {
+        op.xa.geo = d_tables_ + reinterpret_cast<std::intptr_t>(op.xa.geo);
+        if (op.type == Op::Pack) op.xa.lay = dev_layout(op.src_layout);
+        if (op.type == Op::Unpack) op.xa.lay = dev_layout(op.dst_layout);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Execution
+// ---------------------------------------------------------------------------
+void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream) const {
+  if (!on_device_) fail(kErrInvalidArgument, "plan was created by dfft_plan_analyze and cannot execute");
+  if (!in || !out) fail(kErrInvalidArgument, "null buffer");
+  if (in == out) fail(kErrInvalidArgument, "in-place execution is not supported: in and out must differ");
+  auto buf = [&](int id) -> void* {
+    if (id == kBufIn) return const_cast<void*>(in);
+    if (id == kBufOut) return out;
+    return bufs_.at(id);
+  };
+  for (const Op& op0 : prog_[forward ? 0 : 1]) {
+    cudaError_t e = cudaSuccess;
+    switch (op0.type) {
+      case Op::Stage: {
+        if (op0.tiles == 0) break;
+        dev::StageArgs A = op0.sa;
+        A.in = buf(op0.src);
+        A.out = buf(op0.dst);
+        e = dev::launch_fft_stage(A, d_.dbl, op0.kind, op0.inverse, op0.nthreads, op0.smem, op0.tiles, stream);
+        break;
+      }
+      case Op::Pack:
+      case Op::All2All:
+      case Op::Unpack: {
+        dev::XposeArgs X = op0.xa;
+        X.src = buf(op0.src);
+        X.dst = buf(op0.dst);
+        if (X.bufsize * X.nprocs == 0) break;
+        e = dev::launch_xpose(op0.type == Op::Pack ? 0 : (op0.type == Op::All2All ? 1 : 2), X, op0.elem_bytes, stream);
+        break;
+      }
+      case Op::Scale: e = dev::launch_scale(buf(op0.dst), op0.n_real, d_.dbl, op0.scale, stream); break;
+    }
+    if (e != cudaSuccess) fail(kErrCuda, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+  }
+}
+
+void Plan::export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const {
+  if (!on_device_) fail(kErrInvalidArgument, "plan has no device buffers");
+  auto it = debug_bufs_.find({forward ? 0 : 1, static_cast<int>(block * 2 + (which ? 1 : 0))});
+  if (it == debug_bufs_.end())
+    fail(kErrInvalidArgument, "no recorded buffers for this block (literal execution of a transpose block only)");
+  const std::size_t bytes = buf_bytes_.at(it->second);
+  if (capacity < bytes) fail(kErrInvalidArgument, "host buffer too small: need " + std::to_string(bytes) + " bytes");
+  cuda_check(cudaDeviceSynchronize(), "synchronize before export");
+  cuda_check(cudaMemcpy(host, bufs_.at(it->second), bytes, cudaMemcpyDeviceToHost), "export copy");
+}
+
+}  // namespace dfft

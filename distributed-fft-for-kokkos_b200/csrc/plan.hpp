@@ -1,0 +1,118 @@
+// Execution plan: validation (internal_plan_factory), per-rank block
+// analyses, and the device programs that execute the forward and backward
+// transforms.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dev_types.h"
+#include "layout.hpp"
+#include "plan_core.hpp"
+
+namespace dfft {
+
+struct PlanDesc {
+  Ext axes;  // non-negative
+  Ext gin, gout, in_topo, out_topo;
+  bool in_right = true, out_right = true, view_right = true;
+  bool r2c = false;
+  bool dbl = true;
+  int norm = 0;       // 0 backward, 1 forward, 2 ortho, 3 none
+  int exec_mode = 0;  // 0 fused, 1 literal
+  cudaStream_t stream = nullptr;
+};
+
+// Buffer ids used by the device programs.
+enum : int { kBufIn = 0, kBufOut = 1, kBufScratch0 = 2, kBufScratch1 = 3, kBufFirstDebug = 4 };
+
+struct Op {
+  enum Type { Stage, Pack, All2All, Unpack, Scale } type;
+  int src = -1, dst = -1;  // buffer ids
+  // Stage
+  dev::StageArgs sa{};
+  int kind = 0;
+  bool inverse = false;
+  int nthreads = 256;
+  std::size_t smem = 0;
+  unsigned tiles = 0;
+  int src_layout = -1, dst_layout = -1;
+  // Pack / All2All / Unpack
+  dev::XposeArgs xa{};
+  int elem_bytes = 0;
+  int block = -1;  // transpose block index in the block list
+  // Scale
+  std::int64_t n_real = 0;
+  double scale = 1.0;
+};
+
+class Plan {
+ public:
+  Plan(const PlanDesc& d, bool on_device);
+  ~Plan();
+  Plan(const Plan&) = delete;
+  Plan& operator=(const Plan&) = delete;
+
+  void execute(const void* in, void* out, bool forward, cudaStream_t stream) const;
+
+  const std::string& name() const { return name_; }
+  std::size_t nprocs() const { return total_size(d_.in_topo); }
+  const PlanDesc& desc() const { return d_; }
+  const std::vector<BlockAnalyses>& analyses() const { return per_rank_; }
+  std::size_t max_buffer_size() const { return max_buffer_size_; }
+  const std::vector<Ext>& chain() const { return chain_; }
+  const std::vector<std::size_t>& chain_trans_axes() const { return trans_axes_; }
+  const std::vector<std::size_t>& chain_layouts() const { return chain_layouts_; }
+  const Layout& in_layout() const { return lin_; }
+  const Layout& out_layout() const { return lout_; }
+  std::size_t launches(bool forward) const { return prog_[forward ? 0 : 1].size(); }
+  std::size_t workspace_bytes() const { return workspace_bytes_; }
+  bool on_device() const { return on_device_; }
+  // Copy the literal-mode send (which=0) / recv (which=1) buffers of transpose
+  // block `block` to host.
+  void export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const;
+
+ private:
+  PlanDesc d_;
+  bool on_device_;
+  std::string name_;
+  TopologyType type_;
+  std::vector<Ext> chain_;
+  std::vector<std::size_t> trans_axes_, chain_layouts_;
+  std::vector<BlockAnalyses> per_rank_;
+  std::size_t max_buffer_size_ = 0;
+  double scale_fwd_ = 1.0, scale_bwd_ = 1.0;
+  Layout lin_, lout_;
+
+  // device programs and resources
+  std::vector<Layout> layouts_;
+  std::vector<LayoutTables> tables_;
+  std::vector<std::int64_t> host_tables_;
+  std::vector<std::int64_t> layout_base_;  // offset of each layout's tables
+  std::int64_t* d_tables_ = nullptr;
+  std::vector<Op> prog_[2];
+  std::vector<void*> bufs_;                 // device buffers by id (in/out are null)
+  std::vector<std::size_t> buf_bytes_;
+  std::map<std::pair<std::size_t, bool>, void*> twiddles_;
+  std::map<std::pair<int, int>, int> debug_bufs_;  // (dir, block*2 + which) -> buffer id
+  std::size_t workspace_bytes_ = 0;
+
+  void analyze();
+  int add_layout(const Layout& L);
+  std::vector<std::size_t> fft_axis_order() const;
+  Layout block_layout(const Ext& topo, bool rank_right, const Ext& map, bool complex) const;
+  Op make_stage(int src_layout, int dst_layout, std::size_t a, int kind, bool inverse, double scale);
+  std::int64_t add_geo(const Layout& L, const BlockInfo& b, std::size_t pc);
+  void build_fused(bool forward);
+  void build_literal(bool forward);
+  void finalize_program(std::vector<Op>& prog, int cur_layout, int cur_buf, const Layout& final_layout,
+                        double scale, bool final_complex);
+  void allocate_device();
+  const void* twiddle(std::size_t n);
+};
+
+}  // namespace dfft

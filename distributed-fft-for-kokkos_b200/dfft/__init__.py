@@ -1,0 +1,18 @@
+"""B200-native distributed 3D FFT execute path (slab / pencil topologies).
+
+Python mirror of the reference's ``KokkosFFT::Distributed`` plan interface on
+top of the C ABI of ``libdfft.so`` (include/dfft.h)."""
+from ._lib import LIB_PATH, lib  # noqa: F401  (loads libdfft.so or raises)
+from .plan import (  # noqa: F401
+    Direction,
+    DistributedFFTError,
+    ExecMode,
+    Normalization,
+    Plan,
+    Status,
+    execute,
+    gather_blocks,
+    scatter_blocks,
+)
+
+__version__ = lib.dfft_version().decode()

@@ -1,0 +1,101 @@
+"""ctypes binding of include/dfft.h (the C ABI of libdfft.so).
+
+The shared library is built in tree (``make -C csrc``) and loaded from this
+directory; there is no fallback implementation, so a missing or unloadable
+library raises at import time.
+"""
+import ctypes
+import os
+
+MAX_RANK = 4
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdfft.so")
+
+
+class PlanDesc(ctypes.Structure):
+    _fields_ = [
+        ("rank", ctypes.c_int32),
+        ("fft_rank", ctypes.c_int32),
+        ("axes", ctypes.c_int32 * 3),
+        ("in_extents", ctypes.c_uint64 * MAX_RANK),
+        ("out_extents", ctypes.c_uint64 * MAX_RANK),
+        ("in_topology", ctypes.c_uint64 * MAX_RANK),
+        ("out_topology", ctypes.c_uint64 * MAX_RANK),
+        ("in_topology_layout_right", ctypes.c_int32),
+        ("out_topology_layout_right", ctypes.c_int32),
+        ("view_layout_right", ctypes.c_int32),
+        ("kind", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("normalization", ctypes.c_int32),
+        ("exec_mode", ctypes.c_int32),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+class BlockInfo(ctypes.Structure):
+    _fields_ = [
+        ("block_type", ctypes.c_int32),
+        ("block_idx", ctypes.c_int32),
+        ("fft_dim", ctypes.c_int32),
+        ("in_axis", ctypes.c_int32),
+        ("out_axis", ctypes.c_int32),
+        ("comm_axis", ctypes.c_int32),
+        ("in_topology", ctypes.c_uint64 * MAX_RANK),
+        ("out_topology", ctypes.c_uint64 * MAX_RANK),
+        ("in_extents", ctypes.c_uint64 * MAX_RANK),
+        ("out_extents", ctypes.c_uint64 * MAX_RANK),
+        ("buffer_extents", ctypes.c_uint64 * (MAX_RANK + 1)),
+        ("in_map", ctypes.c_uint64 * MAX_RANK),
+        ("out_map", ctypes.c_uint64 * MAX_RANK),
+    ]
+
+
+# name -> (restype, argtypes); the complete list of entry points of dfft.h
+SIGNATURES = {
+    "dfft_plan_desc_init": (None, [ctypes.POINTER(PlanDesc)]),
+    "dfft_plan_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PlanDesc)]),
+    "dfft_plan_analyze": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PlanDesc)]),
+    "dfft_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dfft_execute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
+    "dfft_execute_on_stream": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "dfft_plan_name": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "dfft_get_nprocs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_get_local_extents": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                       ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "dfft_get_local_offset": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
+    "dfft_get_buffer_elements": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
+    "dfft_get_num_blocks": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_get_block_info": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(BlockInfo)]),
+    "dfft_get_max_buffer_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "dfft_get_topology_chain": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_uint64),
+                       ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_debug_export_buffers": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
+                       ctypes.c_uint64]),
+    "dfft_get_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_get_workspace_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "dfft_last_error_string": (ctypes.c_char_p, []),
+    "dfft_version": (ctypes.c_char_p, []),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libdfft.so not found at {LIB_PATH}; build it with `make -C distributed-fft-for-kokkos_b200/csrc` "
+            "(or __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()

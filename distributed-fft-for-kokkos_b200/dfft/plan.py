@@ -1,0 +1,282 @@
+"""Python mirror of the reference's distributed plan interface.
+
+Reference API (paths relative to the reference's ``distributed/src/``)::
+
+    KokkosFFT::Distributed::Plan plan(exec, in, out, axes, in_topology,
+                                      out_topology, comm, norm);   // _Plan.hpp:154-181
+    KokkosFFT::Distributed::execute(plan, in, out, direction);     // _Plan.hpp:212-238
+    plan.name();                                                   // _Plan.hpp:200
+
+Here one process drives one GPU and the ranks of the topologies are virtual.
+Instead of per-rank views the plan takes the global extents, and ``execute``
+takes buffers that hold the local blocks of all ranks concatenated in rank
+order (see ``Plan.local_extents`` / ``Plan.local_offset`` and the
+``scatter_blocks`` / ``gather_blocks`` helpers).  Errors raise
+``DistributedFFTError`` with the library's message, like the reference's
+``std::runtime_error``.
+"""
+import ctypes
+import enum
+
+import numpy as np
+
+from ._lib import BlockInfo, PlanDesc, lib, MAX_RANK
+
+
+class Direction(enum.IntEnum):
+    forward = 0
+    backward = 1
+
+
+class Normalization(enum.IntEnum):
+    backward = 0
+    forward = 1
+    ortho = 2
+    none = 3
+
+
+class ExecMode(enum.IntEnum):
+    fused = 0
+    literal = 1
+
+
+class Status(enum.IntEnum):
+    SUCCESS = 0
+    INVALID_ARGUMENT = 1
+    INVALID_TOPOLOGY = 2
+    INVALID_EXTENTS = 3
+    UNSUPPORTED = 4
+    CUDA = 5
+    ALLOC = 6
+    INTERNAL = 7
+    TIMEOUT = 8
+
+
+class DistributedFFTError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{Status(status).name}: {message}")
+        self.status = Status(status)
+
+
+def _check(status):
+    if status != 0:
+        msg = lib.dfft_last_error_string().decode()
+        raise DistributedFFTError(status, msg)
+
+
+def _as_norm(norm):
+    if isinstance(norm, str):
+        return Normalization[norm]
+    return Normalization(norm)
+
+
+def _ptr(x):
+    """Device pointer of a torch tensor, or an int / ctypes pointer as is."""
+    if x is None:
+        return None
+    if hasattr(x, "data_ptr"):
+        return ctypes.c_void_p(x.data_ptr())
+    return ctypes.c_void_p(int(x))
+
+
+class Plan:
+    """Distributed FFT plan over virtual ranks on the current CUDA device.
+
+    Parameters mirror the reference constructor:
+      in_extents / out_extents : global extents of the input / output view
+          (for R2C the input is real and out_extents[last FFT axis] = n // 2 + 1)
+      axes : FFT axes (1 to 3; negative values count from the end)
+      in_topology / out_topology : ranks along each axis
+      real_input : R2C forward / C2R backward plan (else C2C)
+      precision : "float64" or "float32"
+      norm : Normalization (default backward)
+      layout : memory order of the local blocks, "right" (C) or "left" (Fortran)
+      in_topology_layout / out_topology_layout : rank order of the topologies
+      exec_mode : "fused" (default) or "literal" (reference block sequence)
+      stream : CUDA stream handle (int) the plan launches on
+      analyze_only : plan on the host only (no device memory; cannot execute)
+    """
+
+    def __init__(self, in_extents, out_extents, axes, in_topology, out_topology, real_input=False,
+                 precision="float64", norm=Normalization.backward, layout="right", in_topology_layout="right",
+                 out_topology_layout="right", exec_mode="fused", stream=None, analyze_only=False):
+        rank = len(in_extents)
+        if not (len(out_extents) == len(in_topology) == len(out_topology) == rank):
+            raise DistributedFFTError(Status.INVALID_ARGUMENT, "extents and topologies must have the view rank")
+        if rank > MAX_RANK:
+            raise DistributedFFTError(Status.UNSUPPORTED, f"view rank {rank} > {MAX_RANK}")
+        d = PlanDesc()
+        lib.dfft_plan_desc_init(ctypes.byref(d))
+        d.rank = rank
+        axes = list(axes)
+        if not 1 <= len(axes) <= 3:
+            raise DistributedFFTError(Status.INVALID_ARGUMENT, "the Rank of FFT axes must be between 1 and 3")
+        d.fft_rank = len(axes)
+        for i, a in enumerate(axes):
+            d.axes[i] = int(a)
+        for k in range(rank):
+            d.in_extents[k] = int(in_extents[k])
+            d.out_extents[k] = int(out_extents[k])
+            d.in_topology[k] = int(in_topology[k])
+            d.out_topology[k] = int(out_topology[k])
+        d.in_topology_layout_right = 1 if in_topology_layout == "right" else 0
+        d.out_topology_layout_right = 1 if out_topology_layout == "right" else 0
+        d.view_layout_right = 1 if layout == "right" else 0
+        d.kind = 1 if real_input else 0
+        if precision not in ("float64", "float32"):
+            raise DistributedFFTError(Status.INVALID_ARGUMENT, f"unknown precision {precision}")
+        d.precision = 0 if precision == "float64" else 1
+        d.normalization = int(_as_norm(norm))
+        d.exec_mode = int(ExecMode[exec_mode] if isinstance(exec_mode, str) else exec_mode)
+        d.stream = ctypes.c_void_p(int(stream)) if stream else None
+        self._desc = d
+        self.rank = rank
+        self.real_input = bool(real_input)
+        self.precision = precision
+        self.in_extents = tuple(int(x) for x in in_extents)
+        self.out_extents = tuple(int(x) for x in out_extents)
+        self.axes = tuple(int(a) % rank for a in axes)
+        self.in_topology = tuple(int(x) for x in in_topology)
+        self.out_topology = tuple(int(x) for x in out_topology)
+        self.layout = layout
+        self._h = ctypes.c_void_p()
+        fn = lib.dfft_plan_analyze if analyze_only else lib.dfft_plan_create
+        _check(fn(ctypes.byref(self._h), ctypes.byref(d)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dfft_plan_destroy(h)
+            self._h = None
+
+    # -- reference-facing queries ------------------------------------------
+    def name(self):
+        return lib.dfft_plan_name(self._h).decode()
+
+    @property
+    def nprocs(self):
+        n = ctypes.c_int64()
+        _check(lib.dfft_get_nprocs(self._h, ctypes.byref(n)))
+        return n.value
+
+    def local_extents(self, rank, which="in"):
+        """(extents, starts) of a rank's block (compute_local_extents_and_starts)."""
+        e = (ctypes.c_uint64 * MAX_RANK)()
+        s = (ctypes.c_uint64 * MAX_RANK)()
+        _check(lib.dfft_get_local_extents(self._h, rank, 0 if which == "in" else 1, e, s))
+        return tuple(e[:self.rank]), tuple(s[:self.rank])
+
+    def local_offset(self, rank, which="in"):
+        o = ctypes.c_uint64()
+        _check(lib.dfft_get_local_offset(self._h, rank, 0 if which == "in" else 1, ctypes.byref(o)))
+        return o.value
+
+    def buffer_elements(self, which="in"):
+        c = ctypes.c_uint64()
+        _check(lib.dfft_get_buffer_elements(self._h, 0 if which == "in" else 1, ctypes.byref(c)))
+        return c.value
+
+    @property
+    def max_buffer_size(self):
+        c = ctypes.c_uint64()
+        _check(lib.dfft_get_max_buffer_size(self._h, ctypes.byref(c)))
+        return c.value
+
+    def block_infos(self, rank=0):
+        n = ctypes.c_int64()
+        _check(lib.dfft_get_num_blocks(self._h, ctypes.byref(n)))
+        out = []
+        D = self.rank
+        for b in range(n.value):
+            bi = BlockInfo()
+            _check(lib.dfft_get_block_info(self._h, rank, b, ctypes.byref(bi)))
+            out.append(dict(
+                block_type="FFT" if bi.block_type == 1 else "Transpose", block_idx=bi.block_idx,
+                fft_dim=bi.fft_dim, in_axis=bi.in_axis, out_axis=bi.out_axis, comm_axis=bi.comm_axis,
+                in_topology=tuple(bi.in_topology[:D]), out_topology=tuple(bi.out_topology[:D]),
+                in_extents=tuple(bi.in_extents[:D]), out_extents=tuple(bi.out_extents[:D]),
+                buffer_extents=tuple(bi.buffer_extents[:D + 1]), in_map=tuple(bi.in_map[:D]),
+                out_map=tuple(bi.out_map[:D])))
+        return out
+
+    def topology_chain(self):
+        n = ctypes.c_int64(0)
+        _check(lib.dfft_get_topology_chain(self._h, ctypes.byref(n), None, None, None))
+        cnt = n.value
+        topos = (ctypes.c_uint64 * (cnt * self.rank))()
+        tr = (ctypes.c_int64 * max(cnt, 1))()
+        lay = (ctypes.c_int64 * max(cnt, 1))()
+        _check(lib.dfft_get_topology_chain(self._h, ctypes.byref(n), topos, tr, lay))
+        t = [tuple(topos[i * self.rank:(i + 1) * self.rank]) for i in range(cnt)]
+        return t, list(tr[:max(cnt - 1, 0)]), list(lay[:cnt])
+
+    def launch_count(self, direction=Direction.forward):
+        n = ctypes.c_int64()
+        _check(lib.dfft_get_launch_count(self._h, int(direction), ctypes.byref(n)))
+        return n.value
+
+    def workspace_bytes(self):
+        n = ctypes.c_uint64()
+        _check(lib.dfft_get_workspace_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def export_buffers(self, direction, block, which):
+        """All ranks' send ('send') or recv ('recv') buffers of a transpose block,
+        recorded by the last literal-mode execute; shape (nprocs, *buffer_extents)."""
+        bi = self.block_infos(0)[block]
+        if bi["block_type"] != "Transpose":
+            raise DistributedFFTError(Status.INVALID_ARGUMENT, "not a transpose block")
+        # element type of the exchanged data: real only before the first FFT
+        real = self.real_input and all(b["block_type"] == "Transpose" for b in self.block_infos(0)[:block])
+        dt = (np.float64 if real else np.complex128) if self.precision == "float64" else \
+            (np.float32 if real else np.complex64)
+        bext = tuple(bi["buffer_extents"])
+        per_rank = int(np.prod(bext))
+        flat = np.zeros(self.nprocs * per_rank, dtype=dt)
+        _check(lib.dfft_debug_export_buffers(self._h, int(direction), block, 0 if which == "send" else 1,
+                                             flat.ctypes.data_as(ctypes.c_void_p), flat.nbytes))
+        order = "C" if self.layout == "right" else "F"
+        return np.stack([flat[r * per_rank:(r + 1) * per_rank].reshape(bext, order=order)
+                         for r in range(self.nprocs)])
+
+
+def execute(plan, in_buf, out_buf, direction, stream=None):
+    """execute(plan, in, out, direction) on concatenated per-rank buffers.
+
+    Forward: ``in_buf`` holds the input layout, ``out_buf`` receives the output
+    layout.  Backward: ``in_buf`` holds the (complex) output layout and
+    ``out_buf`` receives the input layout.  Asynchronous on the plan's stream
+    (or ``stream``)."""
+    direction = Direction(direction)
+    if stream is None:
+        _check(lib.dfft_execute(plan._h, _ptr(in_buf), _ptr(out_buf), int(direction)))
+    else:
+        _check(lib.dfft_execute_on_stream(plan._h, _ptr(in_buf), _ptr(out_buf), int(direction),
+                                          ctypes.c_void_p(int(stream))))
+
+
+def scatter_blocks(plan, global_array, which="in"):
+    """Concatenate the per-rank blocks of a global (numpy) array in rank order,
+    each block in the plan's memory order."""
+    a = np.asarray(global_array)
+    parts = []
+    for r in range(plan.nprocs):
+        ext, st = plan.local_extents(r, which)
+        sl = tuple(slice(s, s + e) for s, e in zip(st, ext))
+        blk = a[sl]
+        parts.append(np.ravel(blk, order="C" if plan.layout == "right" else "F"))
+    return np.concatenate(parts) if parts else np.zeros(0, a.dtype)
+
+
+def gather_blocks(plan, flat, which="in", dtype=None):
+    """Inverse of scatter_blocks: rebuild the global (numpy) array."""
+    flat = np.asarray(flat)
+    shape = plan.in_extents if which == "in" else plan.out_extents
+    out = np.zeros(shape, dtype=dtype or flat.dtype)
+    for r in range(plan.nprocs):
+        ext, st = plan.local_extents(r, which)
+        off = plan.local_offset(r, which)
+        n = int(np.prod(ext))
+        blk = flat[off:off + n].reshape(ext, order="C" if plan.layout == "right" else "F")
+        out[tuple(slice(s, s + e) for s, e in zip(st, ext))] = blk
+    return out

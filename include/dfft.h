@@ -1,0 +1,195 @@
+/*
+ * dfft.h - C ABI of the B200-native distributed 3D FFT execute path.
+ *
+ * One process drives one GPU.  The ranks of a slab or pencil topology are
+ * virtual: every buffer handed to dfft_execute holds the local blocks of all
+ * ranks of the topology, concatenated in rank order (rank 0 first), each block
+ * in exactly the shape and memory order that rank holds in the reference
+ * library (see dfft_get_local_extents / dfft_get_local_offset).  The
+ * all-to-all exchanges between the FFT stages become on-device permutations.
+ *
+ * Every entry point returns a dfft_status; nothing throws across the ABI.
+ * dfft_last_error_string() gives the message of the last failure on the
+ * calling thread.
+ *
+ * Reference interfaces replaced (paths relative to the reference's
+ * distributed/src/):
+ *   KokkosFFT::Distributed::Plan ctor        KokkosFFT_Distributed_Plan.hpp:154-181
+ *   internal_plan_factory                    KokkosFFT_Distributed_Plan.hpp:46-113
+ *   KokkosFFT::Distributed::execute          KokkosFFT_Distributed_Plan.hpp:212-238
+ *   Plan::name                               KokkosFFT_Distributed_Plan.hpp:200
+ *   compute_local_extents_and_starts         KokkosFFT_Distributed_MPI_Extents.hpp:546-577
+ *   BlockInfo / block analyses               KokkosFFT_Distributed_Types.hpp:61-154,
+ *                                            KokkosFFT_Distributed_BlockAnalyses.hpp:391-506
+ *   get_all_slab/pencil_topologies           KokkosFFT_Distributed_Topologies.hpp:421-811
+ *   TransBlock pack/all2all/unpack buffers   KokkosFFT_Distributed_TransBlock.hpp:76-107
+ */
+#ifndef DFFT_H
+#define DFFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFFT_MAX_RANK 4
+
+typedef enum {
+  DFFT_SUCCESS = 0,
+  DFFT_ERROR_INVALID_ARGUMENT = 1,
+  DFFT_ERROR_INVALID_TOPOLOGY = 2,
+  DFFT_ERROR_INVALID_EXTENTS = 3,
+  DFFT_ERROR_UNSUPPORTED = 4,
+  DFFT_ERROR_CUDA = 5,
+  DFFT_ERROR_ALLOC = 6,
+  DFFT_ERROR_INTERNAL = 7,
+  DFFT_ERROR_TIMEOUT = 8
+} dfft_status;
+
+/* Transform kind.  R2C plans run C2R on dfft_execute(..., DFFT_BACKWARD). */
+typedef enum { DFFT_KIND_C2C = 0, DFFT_KIND_R2C = 1 } dfft_kind;
+
+/* Storage and arithmetic precision: complex128/float64 or complex64/float32. */
+typedef enum { DFFT_PREC_F64 = 0, DFFT_PREC_F32 = 1 } dfft_precision;
+
+/* KokkosFFT::Normalization (default backward: 1/N on the backward transform). */
+typedef enum {
+  DFFT_NORM_BACKWARD = 0,
+  DFFT_NORM_FORWARD = 1,
+  DFFT_NORM_ORTHO = 2,
+  DFFT_NORM_NONE = 3
+} dfft_normalization;
+
+typedef enum { DFFT_FORWARD = 0, DFFT_BACKWARD = 1 } dfft_direction;
+
+/* Execution strategy.
+ *   DFFT_EXEC_FUSED   : one kernel per FFT axis; pack, all-to-all, unpack,
+ *                       local transposes and normalisation are folded into the
+ *                       loads and stores of those kernels (default).
+ *   DFFT_EXEC_LITERAL : the reference's block sequence kernel by kernel (local
+ *                       transposes, per-axis FFTs, pack, all-to-all
+ *                       permutation, unpack, normalisation pass).  The per-rank
+ *                       send/recv buffers of every transpose block are kept and
+ *                       can be read back with dfft_debug_export_buffers. */
+typedef enum { DFFT_EXEC_FUSED = 0, DFFT_EXEC_LITERAL = 1 } dfft_exec_mode;
+
+typedef struct {
+  int32_t rank;                         /* view rank, 2..4 */
+  int32_t fft_rank;                     /* number of FFT axes, 1..3 */
+  int32_t axes[3];                      /* FFT axes (negative values count from the end) */
+  uint64_t in_extents[DFFT_MAX_RANK];   /* global extents of the input (real extents for R2C) */
+  uint64_t out_extents[DFFT_MAX_RANK];  /* global extents of the (complex) output */
+  uint64_t in_topology[DFFT_MAX_RANK];  /* ranks along each axis for the input */
+  uint64_t out_topology[DFFT_MAX_RANK]; /* ranks along each axis for the output */
+  int32_t in_topology_layout_right;     /* rank order of in_topology: 1 LayoutRight (default), 0 LayoutLeft */
+  int32_t out_topology_layout_right;    /* rank order of out_topology */
+  int32_t view_layout_right;            /* memory order of the local blocks: 1 C order, 0 Fortran order */
+  int32_t kind;                         /* dfft_kind */
+  int32_t precision;                    /* dfft_precision */
+  int32_t normalization;                /* dfft_normalization */
+  int32_t exec_mode;                    /* dfft_exec_mode */
+  void* stream;                         /* cudaStream_t the plan launches on (NULL: legacy default stream) */
+} dfft_plan_desc;
+
+/* One entry of the reference's block list for one virtual rank
+ * (BlockInfo, KokkosFFT_Distributed_Types.hpp:61-154). */
+typedef struct {
+  int32_t block_type; /* 0 Transpose, 1 FFT */
+  int32_t block_idx;
+  int32_t fft_dim;
+  int32_t in_axis, out_axis, comm_axis;
+  uint64_t in_topology[DFFT_MAX_RANK];
+  uint64_t out_topology[DFFT_MAX_RANK];
+  uint64_t in_extents[DFFT_MAX_RANK];
+  uint64_t out_extents[DFFT_MAX_RANK];
+  uint64_t buffer_extents[DFFT_MAX_RANK + 1];
+  uint64_t in_map[DFFT_MAX_RANK];
+  uint64_t out_map[DFFT_MAX_RANK];
+} dfft_block_info;
+
+typedef struct dfft_plan_s dfft_plan;
+
+/* Fill a descriptor with the reference defaults (LayoutRight everywhere,
+ * C2C, F64, backward normalisation, fused execution, legacy stream). */
+void dfft_plan_desc_init(dfft_plan_desc* d);
+
+/* Plan construction (Plan ctor + internal_plan_factory).  Validates the
+ * topologies and extents like the reference and allocates the plan's device
+ * scratch and tables on the current CUDA device. */
+dfft_status dfft_plan_create(dfft_plan** plan, const dfft_plan_desc* desc);
+
+/* Host-only planning: validation and block analyses without touching the GPU.
+ * The returned plan answers the query functions below but cannot execute. */
+dfft_status dfft_plan_analyze(dfft_plan** plan, const dfft_plan_desc* desc);
+
+dfft_status dfft_plan_destroy(dfft_plan* plan);
+
+/* execute(plan, in, out, direction).  Device pointers to concatenated per-rank
+ * blocks.  DFFT_FORWARD reads the input layout from `in` and writes the output
+ * layout to `out`; DFFT_BACKWARD reads the (complex) output layout from `in`
+ * and writes the input layout to `out`.  `in` is not modified.  Asynchronous
+ * on the plan's stream. */
+dfft_status dfft_execute(const dfft_plan* plan, const void* in, void* out, int32_t direction);
+
+/* Same as dfft_execute with an explicit stream (overrides the plan's). */
+dfft_status dfft_execute_on_stream(const dfft_plan* plan, const void* in, void* out, int32_t direction,
+                                   void* stream);
+
+/* "SlabPlan", "PencilPlan" or "SharedPlan" (Plan::name). */
+const char* dfft_plan_name(const dfft_plan* plan);
+
+/* Number of virtual ranks (total size of the topology). */
+dfft_status dfft_get_nprocs(const dfft_plan* plan, int64_t* nprocs);
+
+/* Local extents and starts (logical axis order) of a rank's block; which = 0
+ * input layout, 1 output layout (compute_local_extents_and_starts). */
+dfft_status dfft_get_local_extents(const dfft_plan* plan, int64_t rank, int32_t which, uint64_t* extents,
+                                   uint64_t* starts);
+
+/* Element offset of a rank's block inside the concatenated buffer. */
+dfft_status dfft_get_local_offset(const dfft_plan* plan, int64_t rank, int32_t which, uint64_t* offset);
+
+/* Number of elements (real for an R2C input, complex otherwise) of the
+ * concatenated input (which = 0) or output (which = 1) buffer. */
+dfft_status dfft_get_buffer_elements(const dfft_plan* plan, int32_t which, uint64_t* count);
+
+/* The reference's block list for one virtual rank. */
+dfft_status dfft_get_num_blocks(const dfft_plan* plan, int64_t* nblocks);
+dfft_status dfft_get_block_info(const dfft_plan* plan, int64_t rank, int64_t block, dfft_block_info* info);
+
+/* Max buffer size over ranks in elements of the real type (m_max_buffer_size). */
+dfft_status dfft_get_max_buffer_size(const dfft_plan* plan, uint64_t* size);
+
+/* Topology chain of the slab / pencil analyses.  On entry *n is the capacity
+ * (number of topologies) of the arrays; on return the chain length.
+ * topologies is [n][rank]; trans_axes [n-1] and layouts [n] are pencil-only
+ * (zeros for slabs). */
+dfft_status dfft_get_topology_chain(const dfft_plan* plan, int64_t* n, uint64_t* topologies, int64_t* trans_axes,
+                                    int64_t* layouts);
+
+/* Copy all ranks' send (which = 0) or recv (which = 1) buffers of transpose
+ * block `block` (index in the block list) from the last DFFT_EXEC_LITERAL
+ * execution in `direction` to host memory: nprocs x prod(buffer_extents)
+ * elements, rank-major, each in the reference's buffer order. */
+dfft_status dfft_debug_export_buffers(const dfft_plan* plan, int32_t direction, int64_t block, int32_t which,
+                                      void* host_dst, uint64_t capacity_bytes);
+
+/* Number of kernel launches one dfft_execute issues in a direction. */
+dfft_status dfft_get_launch_count(const dfft_plan* plan, int32_t direction, int64_t* launches);
+
+/* Bytes of device memory the plan holds (scratch, tables, debug buffers). */
+dfft_status dfft_get_workspace_bytes(const dfft_plan* plan, uint64_t* bytes);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* dfft_last_error_string(void);
+
+/* Library version string. */
+const char* dfft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFFT_H */

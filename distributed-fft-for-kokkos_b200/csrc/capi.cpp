@@ -64,7 +64,7 @@ dfft::PlanDesc to_desc(const dfft_plan_desc* d) {
   if (d->kind != DFFT_KIND_C2C && d->kind != DFFT_KIND_R2C) dfft::fail(dfft::kErrInvalidArgument, "unknown kind");
   if (d->precision != DFFT_PREC_F64 && d->precision != DFFT_PREC_F32)
     dfft::fail(dfft::kErrInvalidArgument, "unknown precision");
-  if (d->exec_mode != DFFT_EXEC_FUSED && d->exec_mode != DFFT_EXEC_LITERAL)
+  if (d->exec_mode != DFFT_EXEC_FUSED && d->exec_mode != DFFT_EXEC_LITERAL && d->exec_mode != DFFT_EXEC_LITERAL_CAPTURE)
     dfft::fail(dfft::kErrInvalidArgument, "unknown execution mode");
   p.r2c = d->kind == DFFT_KIND_R2C;
   p.dbl = d->precision == DFFT_PREC_F64;
@@ -274,6 +274,40 @@ dfft_status dfft_get_workspace_bytes(const dfft_plan* plan, uint64_t* bytes) {
   return guarded([&] {
     if (!bytes) dfft::fail(dfft::kErrInvalidArgument, "null output");
     *bytes = impl_of(plan).workspace_bytes();
+  });
+}
+
+dfft_status dfft_get_all_topologies(int32_t pencil, int32_t rank, const uint64_t* in_topology,
+                                    int32_t in_layout_right, const uint64_t* out_topology, int32_t out_layout_right,
+                                    int32_t fft_rank, const int32_t* axes, int64_t* n, uint64_t* topologies,
+                                    int64_t* trans_axes, int64_t* layouts) {
+  return guarded([&] {
+    if (!in_topology || !out_topology || !axes || !n) dfft::fail(dfft::kErrInvalidArgument, "null argument");
+    if (rank < 1 || rank > 8 || fft_rank < 1 || fft_rank > 3) dfft::fail(dfft::kErrInvalidArgument, "bad rank");
+    dfft::Ext in(in_topology, in_topology + rank), out(out_topology, out_topology + rank), ax;
+    for (int i = 0; i < fft_rank; ++i) {
+      int a = axes[i] < 0 ? axes[i] + rank : axes[i];
+      ax.push_back(static_cast<std::size_t>(a));
+    }
+    std::vector<dfft::Ext> chain;
+    std::vector<std::size_t> tr, lay;
+    if (pencil) {
+      auto ch = dfft::get_all_pencil_topologies(in, in_layout_right != 0, out, out_layout_right != 0, ax);
+      chain = ch.topologies;
+      tr = ch.trans_axes;
+      lay = ch.layouts;
+    } else {
+      chain = dfft::get_all_slab_topologies(in, out, ax);
+    }
+    const int64_t cap = *n;
+    *n = static_cast<int64_t>(chain.size());
+    if (cap < *n) return;
+    for (std::size_t i = 0; i < chain.size(); ++i) {
+      if (topologies)
+        for (int k = 0; k < rank; ++k) topologies[i * rank + k] = chain[i][k];
+      if (layouts) layouts[i] = i < lay.size() ? static_cast<int64_t>(lay[i]) : 0;
+      if (trans_axes && i < tr.size()) trans_axes[i] = static_cast<int64_t>(tr[i]);
+    }
   });
 }
 

@@ -77,7 +77,7 @@ Plan::Plan(const PlanDesc& d, bool on_device) : d_(d), on_device_(on_device) {
   try {
     build_fused(true);
     build_fused(false);
-    if (d_.exec_mode == 1) {
+    if (d_.exec_mode == 1 || d_.exec_mode == 2) {
       prog_[0].clear();
       prog_[1].clear();
       build_literal(true);
@@ -412,6 +412,20 @@ std::int64_t Plan::add_geo(const Layout& L, const BlockInfo& b, std::size_t pc) 
   return base;
 }
 
+int Plan::debug_buffer(int dir, std::size_t block, int which, std::size_t bytes) {
+  const auto key = std::make_pair(dir, static_cast<int>(block * 4 + which));
+  auto it = debug_bufs_.find(key);
+  if (it != debug_bufs_.end()) {
+    buf_bytes_[it->second] = std::max(buf_bytes_[it->second], bytes);
+    return it->second;
+  }
+  const int id = static_cast<int>(kBufFirstDebug + debug_bufs_.size());
+  debug_bufs_[key] = id;
+  buf_bytes_.resize(std::max<std::size_t>(buf_bytes_.size(), id + 1), 0);
+  buf_bytes_[id] = bytes;
+  return id;
+}
+
 void Plan::build_literal(bool forward) {
   auto& prog = prog_[forward ? 0 : 1];
   prog.clear();
@@ -456,16 +470,25 @@ void Plan::build_literal(bool forward) {
     const std::size_t pc = d_.view_right ? b.buffer_extents.front() : b.buffer_extents.back();
     const std::size_t bufsize = total_size(b.buffer_extents);
     const int eb = Ls.complex ? (d_.dbl ? 16 : 8) : (d_.dbl ? 8 : 4);
-    // debug send / recv buffers of this block and direction
     std::size_t block_index = 0;
     for (std::size_t i = 0; i < nbl; ++i)
       if (&blocks[i] == &b) block_index = i;
+    const bool capture = d_.exec_mode == 2;
+    const std::size_t xbytes = nprocs() * bufsize * eb;
     int ids[2];
-    for (int w = 0; w < 2; ++w) {
-      ids[w] = static_cast<int>(kBufFirstDebug + debug_bufs_.size());
-      debug_bufs_[{dir, static_cast<int>(block_index * 2 + w)}] = ids[w];
-      buf_bytes_.resize(ids[w] + 1, 0);
-      buf_bytes_[ids[w]] = nprocs() * bufsize * eb;
+    if (capture) {
+      ids[0] = debug_buffer(dir, block_index, 0, xbytes);
+      ids[1] = debug_buffer(dir, block_index, 1, xbytes);
+      Op c;
+      c.type = Op::Copy;
+      c.src = cur_b;
+      c.dst = debug_buffer(dir, block_index, 2, layout_elements(Ls) * eb);
+      c.bytes = layout_elements(Ls) * eb;
+      prog.push_back(c);
+    } else {
+      // send / recv buffers shared by every exchange of the plan
+      ids[0] = debug_buffer(-1, 0, 0, xbytes);
+      ids[1] = debug_buffer(-1, 0, 1, xbytes);
     }
     dev::XposeArgs X;
     std::memset(&X, 0, sizeof(X));
@@ -507,6 +530,14 @@ void Plan::build_literal(bool forward) {
     prog.push_back(unpack);
     cur_l = ld;
     cur_b = unpack.dst;
+    if (capture) {
+      Op c;
+      c.type = Op::Copy;
+      c.src = cur_b;
+      c.dst = debug_buffer(dir, block_index, 3, layout_elements(Ld) * eb);
+      c.bytes = layout_elements(Ld) * eb;
+      prog.push_back(c);
+    }
   };
 
   const int dir = forward ? 0 : 1;
@@ -687,6 +718,7 @@ void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream)
         break;
       }
       case Op::Scale: e = dev::launch_scale(buf(op0.dst), op0.n_real, d_.dbl, op0.scale, stream); break;
+      case Op::Copy: e = cudaMemcpyAsync(buf(op0.dst), buf(op0.src), op0.bytes, cudaMemcpyDeviceToDevice, stream); break;
     }
     if (e != cudaSuccess) fail(kErrCuda, std::string("kernel launch failed: ") + cudaGetErrorString(e));
   }
@@ -694,9 +726,10 @@ void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream)
 
 void Plan::export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const {
   if (!on_device_) fail(kErrInvalidArgument, "plan has no device buffers");
-  auto it = debug_bufs_.find({forward ? 0 : 1, static_cast<int>(block * 2 + (which ? 1 : 0))});
+  if (which < 0 || which > 3) fail(kErrInvalidArgument, "which must be 0 (send), 1 (recv), 2 (pack input) or 3 (unpack output)");
+  auto it = debug_bufs_.find({forward ? 0 : 1, static_cast<int>(block * 4 + which)});
   if (it == debug_bufs_.end())
-    fail(kErrInvalidArgument, "no recorded buffers for this block (literal execution of a transpose block only)");
+    fail(kErrInvalidArgument, "no recorded buffers for this block (capturing literal execution of a transpose block only)");
   const std::size_t bytes = buf_bytes_.at(it->second);
   if (capacity < bytes) fail(kErrInvalidArgument, "host buffer too small: need " + std::to_string(bytes) + " bytes");
   cuda_check(cudaDeviceSynchronize(), "synchronize before export");

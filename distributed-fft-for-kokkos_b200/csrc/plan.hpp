@@ -23,7 +23,7 @@ struct PlanDesc {
   bool r2c = false;
   bool dbl = true;
   int norm = 0;       // 0 backward, 1 forward, 2 ortho, 3 none
-  int exec_mode = 0;  // 0 fused, 1 literal
+  int exec_mode = 0;  // 0 fused, 1 literal, 2 literal with capture of every exchange
   cudaStream_t stream = nullptr;
 };
 
@@ -31,7 +31,7 @@ struct PlanDesc {
 enum : int { kBufIn = 0, kBufOut = 1, kBufScratch0 = 2, kBufScratch1 = 3, kBufFirstDebug = 4 };
 
 struct Op {
-  enum Type { Stage, Pack, All2All, Unpack, Scale } type;
+  enum Type { Stage, Pack, All2All, Unpack, Scale, Copy } type;
   int src = -1, dst = -1;  // buffer ids
   // Stage
   dev::StageArgs sa{};
@@ -45,8 +45,9 @@ struct Op {
   dev::XposeArgs xa{};
   int elem_bytes = 0;
   int block = -1;  // transpose block index in the block list
-  // Scale
+  // Scale / Copy
   std::int64_t n_real = 0;
+  std::size_t bytes = 0;
   double scale = 1.0;
 };
 
@@ -72,8 +73,8 @@ class Plan {
   std::size_t launches(bool forward) const { return prog_[forward ? 0 : 1].size(); }
   std::size_t workspace_bytes() const { return workspace_bytes_; }
   bool on_device() const { return on_device_; }
-  // Copy the literal-mode send (which=0) / recv (which=1) buffers of transpose
-  // block `block` to host.
+  // Copy a buffer recorded by a capturing literal execution of transpose
+  // block `block` to host: which = 0 send, 1 recv, 2 pack input, 3 unpack output.
   void export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const;
 
  private:
@@ -98,7 +99,8 @@ class Plan {
   std::vector<void*> bufs_;                 // device buffers by id (in/out are null)
   std::vector<std::size_t> buf_bytes_;
   std::map<std::pair<std::size_t, bool>, void*> twiddles_;
-  std::map<std::pair<int, int>, int> debug_bufs_;  // (dir, block*2 + which) -> buffer id
+  std::map<std::pair<int, int>, int> debug_bufs_;  // (dir, block*4 + which) -> buffer id
+  int debug_buffer(int dir, std::size_t block, int which, std::size_t bytes);
   std::size_t workspace_bytes_ = 0;
 
   void analyze();

@@ -10,6 +10,7 @@ from .plan import (  # noqa: F401
     Normalization,
     Plan,
     Status,
+    all_topologies,
     execute,
     gather_blocks,
     scatter_blocks,

@@ -80,6 +80,12 @@ SIGNATURES = {
                        ctypes.c_uint64]),
     "dfft_get_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
     "dfft_get_workspace_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "dfft_get_all_topologies": (
+        ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32,
+                       ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32, ctypes.c_int32,
+                       ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64),
+                       ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int64),
+                       ctypes.POINTER(ctypes.c_int64)]),
     "dfft_last_error_string": (ctypes.c_char_p, []),
     "dfft_version": (ctypes.c_char_p, []),
 }

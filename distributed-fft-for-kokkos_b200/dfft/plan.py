@@ -38,6 +38,7 @@ class Normalization(enum.IntEnum):
 class ExecMode(enum.IntEnum):
     fused = 0
     literal = 1
+    literal_capture = 2
 
 
 class Status(enum.IntEnum):
@@ -221,23 +222,68 @@ class Plan:
         return n.value
 
     def export_buffers(self, direction, block, which):
-        """All ranks' send ('send') or recv ('recv') buffers of a transpose block,
-        recorded by the last literal-mode execute; shape (nprocs, *buffer_extents)."""
-        bi = self.block_infos(0)[block]
+        """Data recorded by the last ``exec_mode="literal_capture"`` execute for
+        transpose block ``block``:
+
+        * ``"send"`` / ``"recv"``: all ranks' buffers, shape (nprocs, *buffer_extents)
+          in the reference's buffer order;
+        * ``"pack_in"`` / ``"unpack_out"``: list of every rank's local array (dims
+          in the order of the block's map) that was packed / unpacked."""
+        infos = [self.block_infos(r) for r in range(self.nprocs)]
+        bi = infos[0][block]
         if bi["block_type"] != "Transpose":
             raise DistributedFFTError(Status.INVALID_ARGUMENT, "not a transpose block")
-        # element type of the exchanged data: real only before the first FFT
-        real = self.real_input and all(b["block_type"] == "Transpose" for b in self.block_infos(0)[:block])
+        real = self.real_input and all(b["block_type"] == "Transpose" for b in infos[0][:block])
         dt = (np.float64 if real else np.complex128) if self.precision == "float64" else \
             (np.float32 if real else np.complex64)
-        bext = tuple(bi["buffer_extents"])
-        per_rank = int(np.prod(bext))
-        flat = np.zeros(self.nprocs * per_rank, dtype=dt)
-        _check(lib.dfft_debug_export_buffers(self._h, int(direction), block, 0 if which == "send" else 1,
-                                             flat.ctypes.data_as(ctypes.c_void_p), flat.nbytes))
         order = "C" if self.layout == "right" else "F"
-        return np.stack([flat[r * per_rank:(r + 1) * per_rank].reshape(bext, order=order)
-                         for r in range(self.nprocs)])
+        code = dict(send=0, recv=1, pack_in=2, unpack_out=3)[which]
+        fwd = Direction(direction) == Direction.forward
+        if code < 2:
+            bext = tuple(bi["buffer_extents"])
+            per_rank = int(np.prod(bext))
+            flat = np.zeros(self.nprocs * per_rank, dtype=dt)
+        else:
+            side = "in_extents" if (code == 2) == fwd else "out_extents"
+            shapes = [tuple(infos[r][block][side]) for r in range(self.nprocs)]
+            flat = np.zeros(sum(int(np.prod(s)) for s in shapes), dtype=dt)
+        _check(lib.dfft_debug_export_buffers(self._h, int(direction), block, code,
+                                             flat.ctypes.data_as(ctypes.c_void_p), flat.nbytes))
+        if code < 2:
+            return np.stack([flat[r * per_rank:(r + 1) * per_rank].reshape(bext, order=order)
+                             for r in range(self.nprocs)])
+        out, off = [], 0
+        for s in shapes:
+            n = int(np.prod(s))
+            out.append(flat[off:off + n].reshape(s, order=order))
+            off += n
+        return out
+
+
+def all_topologies(kind, in_topology, out_topology, axes, in_layout="right", out_layout="right"):
+    """get_all_slab_topologies / get_all_pencil_topologies on their own.
+
+    Returns the chain for slabs, and (chain, trans_axes, layouts) for pencils."""
+    rank = len(in_topology)
+    pencil = 1 if kind == "pencil" else 0
+    it = (ctypes.c_uint64 * rank)(*in_topology)
+    ot = (ctypes.c_uint64 * rank)(*out_topology)
+    ax = (ctypes.c_int32 * len(axes))(*axes)
+    n = ctypes.c_int64(0)
+    _check(lib.dfft_get_all_topologies(pencil, rank, it, 1 if in_layout == "right" else 0, ot,
+                                       1 if out_layout == "right" else 0, len(axes), ax, ctypes.byref(n),
+                                       None, None, None))
+    cnt = n.value
+    topos = (ctypes.c_uint64 * (cnt * rank))()
+    tr = (ctypes.c_int64 * max(cnt, 1))()
+    lay = (ctypes.c_int64 * max(cnt, 1))()
+    _check(lib.dfft_get_all_topologies(pencil, rank, it, 1 if in_layout == "right" else 0, ot,
+                                       1 if out_layout == "right" else 0, len(axes), ax, ctypes.byref(n),
+                                       topos, tr, lay))
+    chain = [tuple(topos[i * rank:(i + 1) * rank]) for i in range(cnt)]
+    if not pencil:
+        return chain
+    return chain, list(tr[:max(cnt - 1, 0)]), list(lay[:cnt])
 
 
 def execute(plan, in_buf, out_buf, direction, stream=None):

@@ -65,15 +65,18 @@ typedef enum {
 typedef enum { DFFT_FORWARD = 0, DFFT_BACKWARD = 1 } dfft_direction;
 
 /* Execution strategy.
- *   DFFT_EXEC_FUSED   : one kernel per FFT axis; pack, all-to-all, unpack,
- *                       local transposes and normalisation are folded into the
- *                       loads and stores of those kernels (default).
- *   DFFT_EXEC_LITERAL : the reference's block sequence kernel by kernel (local
- *                       transposes, per-axis FFTs, pack, all-to-all
- *                       permutation, unpack, normalisation pass).  The per-rank
- *                       send/recv buffers of every transpose block are kept and
- *                       can be read back with dfft_debug_export_buffers. */
-typedef enum { DFFT_EXEC_FUSED = 0, DFFT_EXEC_LITERAL = 1 } dfft_exec_mode;
+ *   DFFT_EXEC_FUSED           : one kernel per FFT axis; pack, all-to-all,
+ *                               unpack, local transposes and normalisation are
+ *                               folded into the loads and stores of those
+ *                               kernels (default).
+ *   DFFT_EXEC_LITERAL         : the reference's block sequence kernel by kernel
+ *                               (local transposes, per-axis FFTs, pack,
+ *                               all-to-all permutation, unpack, normalisation).
+ *   DFFT_EXEC_LITERAL_CAPTURE : as DFFT_EXEC_LITERAL, and every transpose
+ *                               block's pack input, send and recv buffers and
+ *                               unpack output are kept for
+ *                               dfft_debug_export_buffers. */
+typedef enum { DFFT_EXEC_FUSED = 0, DFFT_EXEC_LITERAL = 1, DFFT_EXEC_LITERAL_CAPTURE = 2 } dfft_exec_mode;
 
 typedef struct {
   int32_t rank;                         /* view rank, 2..4 */
@@ -169,10 +172,23 @@ dfft_status dfft_get_max_buffer_size(const dfft_plan* plan, uint64_t* size);
 dfft_status dfft_get_topology_chain(const dfft_plan* plan, int64_t* n, uint64_t* topologies, int64_t* trans_axes,
                                     int64_t* layouts);
 
-/* Copy all ranks' send (which = 0) or recv (which = 1) buffers of transpose
- * block `block` (index in the block list) from the last DFFT_EXEC_LITERAL
- * execution in `direction` to host memory: nprocs x prod(buffer_extents)
- * elements, rank-major, each in the reference's buffer order. */
+/* get_all_slab_topologies (pencil = 0) / get_all_pencil_topologies (pencil = 1),
+ * KokkosFFT_Distributed_Topologies.hpp:421-618 / :645-811, on their own.  On
+ * entry *n is the capacity (number of topologies) of the output arrays; on
+ * return the chain length.  topologies is [n][rank], trans_axes [n-1] and
+ * layouts [n] (pencil only).  Fails with DFFT_ERROR_INVALID_TOPOLOGY where the
+ * reference throws. */
+dfft_status dfft_get_all_topologies(int32_t pencil, int32_t rank, const uint64_t* in_topology,
+                                    int32_t in_layout_right, const uint64_t* out_topology, int32_t out_layout_right,
+                                    int32_t fft_rank, const int32_t* axes, int64_t* n, uint64_t* topologies,
+                                    int64_t* trans_axes, int64_t* layouts);
+
+/* Copy data recorded by the last DFFT_EXEC_LITERAL_CAPTURE execution in
+ * `direction` for transpose block `block` (index in the block list) to host:
+ *   which = 0 send buffers, 1 recv buffers: nprocs x prod(buffer_extents)
+ *             elements, rank-major, each in the reference's buffer order;
+ *   which = 2 pack input, 3 unpack output: the concatenated per-rank blocks of
+ *             the block's input / output layout. */
 dfft_status dfft_debug_export_buffers(const dfft_plan* plan, int32_t direction, int64_t block, int32_t which,
                                       void* host_dst, uint64_t capacity_bytes);
 

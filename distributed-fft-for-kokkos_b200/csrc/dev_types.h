@@ -15,7 +15,7 @@ struct DevLayout {
   int64_t off[4], rk[4], loc[4], rbase, rstride;
 };
 
-enum StageKind { kC2C = 0, kR2C = 1, kC2R = 2, kCopy = 3 };
+enum StageKind { kC2C = 0, kR2C = 1, kC2R = 2, kCopy = 3, kCopyReal = 4 };
 
 constexpr int kMaxPasses = 16;
 

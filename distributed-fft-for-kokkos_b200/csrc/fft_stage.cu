@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(256) fft_stage_kernel(const StageArgs A) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) cbase[k] = (k == A.o0) ? co0 : ((k == A.o1) ? co1 : 0);
 
-  if (KIND != kCopy) {
+  if (KIND != kCopy && KIND != kCopyReal) {
     const C* gtw = reinterpret_cast<const C*>(A.tw);
     for (int i = threadIdx.x; i < A.n; i += nt) tw[i] = gtw[i];
   }
@@ -260,6 +260,8 @@ __global__ void __launch_bounds__(256) fft_stage_kernel(const StageArgs A) {
         C v = mk<T>(T(0), T(0));
         if (valid) v = reinterpret_cast<const C*>(A.in)[layout_offset(lsrc, c, A.nd)];
         buf0[(line >> 1) * A.pitch + (line & 1) * na + pos] = v;
+      } else if (KIND == kCopyReal) {
+        if (valid) buf0[line * A.pitch + pos] = mk<T>(reinterpret_cast<const T*>(A.in)[layout_offset(lsrc, c, A.nd)], T(0));
       } else {
         if (valid) buf0[line * A.pitch + pos] = reinterpret_cast<const C*>(A.in)[layout_offset(lsrc, c, A.nd)];
       }
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(256) fft_stage_kernel(const StageArgs A) {
     nxt = buf0;
   }
 
-  if (KIND != kCopy) {
+  if (KIND != kCopy && KIND != kCopyReal) {
     int Ns = 1;
     unsigned long long code = A.radix_code;
     for (int p = 0; p < A.npass; ++p) {
@@ -340,6 +342,8 @@ __global__ void __launch_bounds__(256) fft_stage_kernel(const StageArgs A) {
       } else if (KIND == kC2R) {
         const C z = cur[(line >> 1) * A.pitch + pos];
         reinterpret_cast<T*>(A.out)[o] = ((line & 1) ? z.y : z.x) * s;
+      } else if (KIND == kCopyReal) {
+        reinterpret_cast<T*>(A.out)[o] = cur[line * A.pitch + pos].x * s;
       } else {
         reinterpret_cast<C*>(A.out)[o] = cscale(cur[line * A.pitch + pos], s);
       }
@@ -359,6 +363,7 @@ static cudaError_t launch_stage_t(const StageArgs& A, int kind, bool inverse, in
     case kR2C: k = fft_stage_kernel<T, kR2C, false>; break;
     case kC2R: k = fft_stage_kernel<T, kC2R, true>; break;
     case kCopy: k = fft_stage_kernel<T, kCopy, false>; break;
+    case kCopyReal: k = fft_stage_kernel<T, kCopyReal, false>; break;
     default: return cudaErrorInvalidValue;
   }
   if (smem > 48 * 1024) {

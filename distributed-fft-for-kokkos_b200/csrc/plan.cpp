@@ -281,7 +281,12 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   A.n = static_cast<int>(n);
   A.na_in = static_cast<int>(S.gext[a]);
   A.na_out = static_cast<int>(Dl.gext[a]);
-  if (kind == dev::kCopy && A.na_in != A.na_out) fail(kErrInternal, "copy stage with different extents");
+  if (kind == dev::kCopy && !S.complex) {
+    op.kind = kind = dev::kCopyReal;
+  }
+  const bool is_copy = kind == dev::kCopy || kind == dev::kCopyReal;
+  if (is_copy && (A.na_in != A.na_out || S.complex != Dl.complex))
+    fail(kErrInternal, "copy stage between different extents or element types");
   const std::size_t fs = layout_fast_axis(S), fd = layout_fast_axis(Dl);
   std::size_t b;
   if (fd != a) b = fd;
@@ -300,7 +305,7 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   A.store_afast = fd == a ? 1 : 0;
   A.scale = scale;
 
-  if (kind != dev::kCopy) {
+  if (!is_copy) {
     auto radices = radix_plan(n);
     A.npass = static_cast<int>(radices.size());
     unsigned long long code = 0;
@@ -330,7 +335,7 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   op.tiles = static_cast<unsigned>(tiles);
   op.smem = smem_for(B);
   op.nthreads = 256;
-  if (kind != dev::kCopy) A.tw = twiddle(n);
+  if (!is_copy) A.tw = twiddle(n);
   return op;
 }
 

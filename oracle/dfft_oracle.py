@@ -229,19 +229,22 @@ def all2all(sends, groups, layout_right=True):
 # ---------------------------------------------------------------------------
 def global_fft(x, axes, real_input, norm="backward"):
     """Global forward transform the reference's tests compare against
-    (KokkosFFT::rfftn / fftn with the given normalisation)."""
+    (KokkosFFT::rfftn / fftn with the given normalisation; "none" scales by 1
+    in both directions)."""
     x = np.asarray(x)
+    npn = "backward" if norm == "none" else norm
     if real_input:
-        return np.fft.rfftn(x.astype(np.float64), axes=axes, norm=norm)
-    return np.fft.fftn(x.astype(np.complex128), axes=axes, norm=norm)
+        return np.fft.rfftn(x.astype(np.float64), axes=axes, norm=npn)
+    return np.fft.fftn(x.astype(np.complex128), axes=axes, norm=npn)
 
 
 def global_ifft(X, axes, real_input, real_shape=None, norm="backward"):
     X = np.asarray(X).astype(np.complex128)
+    npn = "forward" if norm == "none" else norm  # "forward" leaves the inverse unscaled
     if real_input:
         s = [real_shape[a] for a in axes]
-        return np.fft.irfftn(X, s=s, axes=axes, norm=norm)
-    return np.fft.ifftn(X, axes=axes, norm=norm)
+        return np.fft.irfftn(X, s=s, axes=axes, norm=npn)
+    return np.fft.ifftn(X, axes=axes, norm=npn)
 
 
 def naive_dftn(x, axes, sign=-1):

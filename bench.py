@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark of the distributed 3D FFT execute path on B200.
+
+Workload (one step): forward + backward 512^3 C2C transform in complex64 on a
+pencil topology (4,4,1) -> (1,4,4) of 16 virtual ranks, fused execution.
+Every GPU (rank) runs its own field ("weak" scaling, no data-path collective:
+the virtual ranks of a topology live on one GPU).
+
+Reported:
+  value      whole-job algorithmic HBM throughput in GB/s: per direction one
+             read + one write of the field per axis stage (3 stages), i.e.
+             12 * N * 8 bytes per step, over the device time of the step
+  gflops     5 N log2 N flops per complex transform direction
+  fp64_*     the plain FP64 path (same plan, complex128) and the time ratio
+  e2e        the same metric through the C ABI with host buffers: pinned
+             host -> device copy of the input, forward, backward, device ->
+             host copy of the result, every step
+  roofline   the FFT stage kernel (every launch of the step) against the
+             measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (numpy restatement of the reference block walk)
+             on a bounded 256^3 sample, rank 0 only
+
+``--impl reference`` times the CPU restatement of the reference's execute
+path (the reference itself cannot be built here: Kokkos, kokkos-fft, FFTW and
+MPI are absent) on the host with all available threads.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "distributed-fft-for-kokkos_b200"))
+
+N_EDGE = 512
+TOPO_IN, TOPO_OUT = (4, 4, 1), (1, 4, 4)
+CPU_SAMPLE_EDGE = 256
+WORKLOAD = (f"{N_EDGE}^3 C2C complex64 forward+backward, pencil {TOPO_IN}->{TOPO_OUT} "
+            f"(16 virtual ranks on one GPU), fused")
+METRIC = "3D FFT fwd+bwd algorithmic HBM throughput"
+
+
+def algo_bytes(n, elem):
+    # per direction: 3 axis stages x (read + write) of n^3 elements
+    return 2 * 3 * 2 * n ** 3 * elem
+
+
+def flops(n):
+    N = n ** 3
+    return 2 * 5 * N * math.log2(N)
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def start_clock_sampler(device):
+    fd, path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+    os.close(fd)
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                              "-lms", "200"], stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        p = None
+    return p, path
+
+
+def stop_clock_sampler(p, path):
+    if p is not None:
+        p.terminate()
+        try:
+            p.wait(timeout=5)
+        except Exception:
+            p.kill()
+    sm, mx, reasons = [], None, set()
+    try:
+        for line in open(path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+    finally:
+        try:
+            os.remove(path)
+        except OSError:
+            pass
+    sm.sort()
+    return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def cpu_baseline(steps=2, workers=None):
+    """CPU oracle on a bounded sample (256^3 complex64, same topology)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+
+    import dfft
+    import dfft_oracle as O
+    from _plan_info import plan_info
+
+    n = CPU_SAMPLE_EDGE
+    p = dfft.Plan((n,) * 3, (n,) * 3, (0, 1, 2), TOPO_IN, TOPO_OUT, precision="float32", analyze_only=True)
+    info = plan_info(p)
+    rng = np.random.default_rng(1)
+    x = (rng.standard_normal((n,) * 3) + 1j * rng.standard_normal((n,) * 3)).astype(np.complex64)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        y = O.execute_literal(x, info, True, workers=workers)
+        O.execute_literal(y, info, False, workers=workers)
+    dt = (time.perf_counter() - t0) / steps
+    return {
+        "value": round(algo_bytes(n, 8) / dt / 1e9, 3), "unit": "GB/s", "cores": workers or 1, "kind": "port",
+        "ms_per_step": round(dt * 1e3, 1),
+        "sample": f"{n}^3 C2C complex64 fwd+bwd, pencil {TOPO_IN}->{TOPO_OUT}, numpy restatement of the "
+                  f"reference block walk (pocketfft local FFTs, pack/all2all/unpack), {steps} steps"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    workers = os.cpu_count() or 1
+    cpu_baseline(steps=1, workers=workers)  # warm-up (imports, allocator)
+    res = []
+    for _ in range(max(1, args.steps)):
+        res.append(cpu_baseline(steps=1, workers=workers))
+    v = sorted(r["value"] for r in res)[len(res) // 2]
+    cb = dict(res[0])
+    cb["value"] = v
+    cb["sample"] += f" (median of {len(res)} timed steps after 1 warm-up)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{CPU_SAMPLE_EDGE}^3 C2C complex64 forward+backward, pencil {TOPO_IN}->{TOPO_OUT}, "
+                               "CPU restatement of the reference execute path"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+
+    import dfft
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = N_EDGE
+    g = (n, n, n)
+    stream = torch.cuda.current_stream()
+
+    def make(precision):
+        return dfft.Plan(g, g, (0, 1, 2), TOPO_IN, TOPO_OUT, precision=precision, stream=stream.cuda_stream)
+
+    def timed(plan, a, b, c, steps):
+        for _ in range(args.warmup):
+            dfft.execute(plan, a, b, dfft.Direction.forward)
+            dfft.execute(plan, b, c, dfft.Direction.backward)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            dfft.execute(plan, a, b, dfft.Direction.forward)
+            dfft.execute(plan, b, c, dfft.Direction.backward)
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    # ---- FP32 fused path (headline) ----
+    p32 = make("float32")
+    a32 = torch.randn(n ** 3, dtype=torch.complex64, device="cuda", generator=gen)
+    b32 = torch.empty_like(a32)
+    c32 = torch.empty_like(a32)
+    sampler = start_clock_sampler(local)
+    ms32 = max_over_ranks(timed(p32, a32, b32, c32, args.steps))
+    clocks = stop_clock_sampler(*sampler)
+    launches = p32.launch_count(dfft.Direction.forward) + p32.launch_count(dfft.Direction.backward)
+
+    # ---- plain FP64 path and the error of the FP32 result ----
+    p64 = make("float64")
+    a64 = a32.to(torch.complex128)
+    b64 = torch.empty_like(a64)
+    c64 = torch.empty_like(a64)
+    ms64 = max_over_ranks(timed(p64, a64, b64, c64, max(3, args.steps // 2)))
+    dfft.execute(p32, a32, b32, dfft.Direction.forward)
+    dfft.execute(p64, a64, b64, dfft.Direction.forward)
+    torch.cuda.synchronize()
+    err_fwd = float(torch.linalg.vector_norm(b32.to(torch.complex128) - b64) / torch.linalg.vector_norm(b64))
+    err_rt = float(torch.linalg.vector_norm(c32.to(torch.complex128) - a64) / torch.linalg.vector_norm(a64))
+    del a64, b64, c64, p64
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the C ABI with host buffers ----
+    h_in = a32.cpu().pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        a32.copy_(h_in, non_blocking=True)
+        dfft.execute(p32, a32, b32, dfft.Direction.forward)
+        dfft.execute(p32, b32, c32, dfft.Direction.backward)
+        h_out.copy_(c32, non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        a32.copy_(h_in, non_blocking=True)
+        dfft.execute(p32, a32, b32, dfft.Direction.forward)
+        dfft.execute(p32, b32, c32, dfft.Direction.backward)
+        h_out.copy_(c32, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+
+    step_bytes = algo_bytes(n, 8)
+    value = world * step_bytes / (ms32 * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    per_launch_bytes = step_bytes / launches
+    launch_ms = ms32 / launches
+    achieved = per_launch_bytes / (launch_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            traffic = json.load(f).get("fft_stage_512_c64_per_launch_bytes")
+    except Exception:
+        pass
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms32, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (complex N(0,1), torch generator seed 1234+rank)",
+            "config": {"workload": WORKLOAD, "n": n, "topology_in": list(TOPO_IN), "topology_out": list(TOPO_OUT),
+                       "precision": "complex64", "exec_mode": "fused",
+                       "l2": "inputs (1 GiB per field) larger than the 126 MB L2",
+                       "parallelism": f"weak, one 512^3 field per GPU x {world}"},
+            "gflops": round(world * flops(n) / (ms32 * 1e-3) / 1e9, 1),
+            "fp64_ms_per_step": round(ms64, 4),
+            "fp32_over_fp64_speedup": round(ms64 / ms32, 3),
+            "rel_l2_fp32_vs_fp64_forward": err_fwd,
+            "rel_l2_fp32_roundtrip": err_rt,
+            "e2e": {"value": round(world * step_bytes / (ms_e2e * 1e-3) / 1e9, 2), "unit": "GB/s",
+                    "ms_per_step": round(ms_e2e, 3), "h2d_bytes_per_step": int(h_in.numel() * 8),
+                    "d2h_bytes_per_step": int(h_out.numel() * 8)},
+            "roofline": {"bound": "hbm", "kernel": "fft_stage_kernel (every launch of the step)",
+                         "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "algorithmic_bytes_per_launch": int(per_launch_bytes)},
+            "clocks": clocks,
+            "gpu_launches": int(launches * args.steps),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(steps=2)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

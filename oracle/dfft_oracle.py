@@ -268,23 +268,28 @@ def rel_l2(a, b):
 # ---------------------------------------------------------------------------
 # literal execution of the reference block sequence with virtual ranks
 # ---------------------------------------------------------------------------
-def _local_fft(x, fft_dim, first_fft, real_input, forward, layout_right, real_len=None):
+def _local_fft(x, fft_dim, first_fft, real_input, forward, layout_right, real_len=None, workers=None):
     D = x.ndim
     dims = list(range(D - fft_dim, D)) if layout_right else list(range(fft_dim))[::-1]
-    # numpy transforms the last entry of `axes` as the real one: make it the
+    # the last entry of `axes` is transformed as the real one: make it the
     # innermost (unit-stride) dim
+    if workers:
+        import scipy.fft as F  # pocketfft with a thread pool
+        kw = dict(workers=workers)
+    else:
+        F, kw = np.fft, {}
     if forward:
         if first_fft and real_input:
-            return np.fft.rfftn(x, axes=dims)
-        return np.fft.fftn(x, axes=dims)
+            return F.rfftn(x, axes=dims, **kw)
+        return F.fftn(x, axes=dims, **kw)
     if first_fft and real_input:
         s = [x.shape[d] for d in dims]
         s[-1] = real_len
-        return np.fft.irfftn(x, s=s, axes=dims) * np.prod(s)
-    return np.fft.ifftn(x, axes=dims) * np.prod([x.shape[d] for d in dims])
+        return F.irfftn(x, s=s, axes=dims, **kw) * np.prod(s)
+    return F.ifftn(x, axes=dims, **kw) * np.prod([x.shape[d] for d in dims])
 
 
-def execute_literal(x_global, plan_info, forward=True, record=None):
+def execute_literal(x_global, plan_info, forward=True, record=None, workers=None):
     """Run the reference block walk on the host.
 
     ``plan_info``: dict with keys in_extents, out_extents, axes, in_topology,
@@ -333,7 +338,7 @@ def execute_literal(x_global, plan_info, forward=True, record=None):
                     loc = [np.ascontiguousarray(np.transpose(np.transpose(l, np.argsort(cur_map)), b["in_map"]))
                            for l in loc]
                     cur_map = tuple(b["in_map"])
-                loc = [_local_fft(l, b["fft_dim"], n_fft == 0, real, True, right) for l in loc]
+                loc = [_local_fft(l, b["fft_dim"], n_fft == 0, real, True, right, workers=workers) for l in loc]
                 n_fft += 1
             else:
                 pencil = pi["pencil"]
@@ -373,7 +378,7 @@ def execute_literal(x_global, plan_info, forward=True, record=None):
             if first and real:
                 inner = b["in_map"][-1] if right else b["in_map"][0]
                 real_len = gin[inner]
-            loc = [_local_fft(l, b["fft_dim"], first, real, False, right, real_len) for l in loc]
+            loc = [_local_fft(l, b["fft_dim"], first, real, False, right, real_len, workers=workers) for l in loc]
         else:
             pencil = pi["pencil"]
             groups = exchange_groups(pi["in_topology"], P, b["comm_axis"], pencil)

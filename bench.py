@@ -151,8 +151,10 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{CPU_SAMPLE_EDGE}^3 C2C complex64 forward+backward, pencil {TOPO_IN}->{TOPO_OUT}, "
-                               "CPU restatement of the reference execute path"},
+        "config": {"workload": WORKLOAD, "n": N_EDGE, "topology_in": list(TOPO_IN), "topology_out": list(TOPO_OUT),
+                   "precision": "complex64",
+                   "sample": f"each step is a bounded {CPU_SAMPLE_EDGE}^3 sample of the workload on the host CPU "
+                             "(CPU restatement of the reference execute path)"},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -62,6 +62,12 @@ struct XposeArgs {
 
 cudaError_t launch_fft_stage(const StageArgs& A, bool dbl, int kind, bool inverse, int nthreads, size_t smem,
                              unsigned tiles, cudaStream_t st);
+// Register-resident power-of-two stage (fft_fast.cu): line lengths 16..4096,
+// C2C, rows contiguous on both sides.
+bool fast_stage_supported(int n);
+int fast_stage_lines(bool dbl, int n);
+cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, unsigned tiles,
+                            cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
 cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);

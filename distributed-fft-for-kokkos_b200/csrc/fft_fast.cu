@@ -1,0 +1,340 @@
+// Register-resident FFT stage for power-of-two lines (sm_100a).
+//
+// Used when both the source and the destination address every tile row as a
+// contiguous run: either every line is contiguous (unit stride along the FFT
+// axis a, "a-fast") or, for every position along a, the B lines of the tile
+// are contiguous (unit stride along the tile axis b, "b-fast").  Per-row base
+// offsets come from the separable layout tables, so the stage still performs
+// the reference's pack / all-to-all / unpack / local transpose by addressing.
+//
+// Each line of length N is transformed by N/8 threads holding 8 values each.
+// The first radix pass reads its inputs straight from global memory and the
+// last pass writes its outputs straight to global memory (consecutive threads
+// touch consecutive addresses for either row orientation); the passes in
+// between exchange values through padded shared memory (one pad element per
+// 256 bytes, which keeps the stride-R Stockham writes conflict-light).
+#include "fft_stage.cuh"
+
+namespace dfft {
+namespace dev {
+
+namespace {
+
+template <bool INV, typename C>
+__device__ __forceinline__ void r4(C& v0, C& v1, C& v2, C& v3) {
+  C s02 = cadd(v0, v2), d02 = csub(v0, v2);
+  C s13 = cadd(v1, v3), d13 = rot<INV>(csub(v1, v3));
+  v0 = cadd(s02, s13);
+  v2 = csub(s02, s13);
+  v1 = cadd(d02, d13);
+  v3 = csub(d02, d13);
+}
+
+template <typename T, bool INV>
+__device__ __forceinline__ void r8(cplx<T>* v) {
+  using C = cplx<T>;
+  const T h = T(0.70710678118654752440084436210484903928);
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  r4<INV>(e0, e1, e2, e3);
+  r4<INV>(o0, o1, o2, o3);
+  C t1, t3;
+  if (INV) {
+    t1 = mk<T>(h * (o1.x - o1.y), h * (o1.x + o1.y));
+    t3 = mk<T>(-h * (o3.x + o3.y), h * (o3.x - o3.y));
+  } else {
+    t1 = mk<T>(h * (o1.x + o1.y), h * (o1.y - o1.x));
+    t3 = mk<T>(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+  }
+  C t2 = rot<INV>(o2);
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, t1);
+  v[5] = csub(e1, t1);
+  v[2] = cadd(e2, t2);
+  v[6] = csub(e2, t2);
+  v[3] = cadd(e3, t3);
+  v[7] = csub(e3, t3);
+}
+
+template <typename T, bool INV, int R>
+__device__ __forceinline__ void dftR(cplx<T>* v) {
+  if constexpr (R == 2) {
+    const cplx<T> t = v[0];
+    v[0] = cadd(t, v[1]);
+    v[1] = csub(t, v[1]);
+  } else if constexpr (R == 4) {
+    r4<INV>(v[0], v[1], v[2], v[3]);
+  } else {
+    r8<T, INV>(v);
+  }
+}
+
+// radix of pass P of an N-point plan: the first and the last pass are radix 8
+// whenever N allows it; all radices divide 8.
+template <int N, int P>
+struct Radix;
+#define DFFT_PLAN(N_, ...)                                       \
+  template <int P>                                               \
+  struct Radix<N_, P> {                                          \
+    static constexpr int list[] = {__VA_ARGS__};                 \
+    static constexpr int npass = sizeof(list) / sizeof(int);     \
+    static constexpr int value = P < npass ? list[P < npass ? P : 0] : 1; \
+  };
+DFFT_PLAN(16, 2, 8)
+DFFT_PLAN(32, 4, 8)
+DFFT_PLAN(64, 8, 8)
+DFFT_PLAN(128, 8, 2, 8)
+DFFT_PLAN(256, 8, 4, 8)
+DFFT_PLAN(512, 8, 8, 8)
+DFFT_PLAN(1024, 8, 4, 4, 8)
+DFFT_PLAN(2048, 8, 4, 8, 8)
+DFFT_PLAN(4096, 8, 8, 8, 8)
+#undef DFFT_PLAN
+
+template <int N, int P>
+struct NsOf {
+  static constexpr int value = NsOf<N, P - 1>::value * Radix<N, P - 1>::value;
+};
+template <int N>
+struct NsOf<N, 0> {
+  static constexpr int value = 1;
+};
+
+// padded shared-memory position: one pad element per 256 bytes
+template <typename T>
+__device__ __forceinline__ int padpos(int p) {
+  return sizeof(T) == 4 ? p + (p >> 5) : p + (p >> 4);
+}
+
+// element position of value (q, r) of thread t at the input of pass P
+template <int N, int P, int TT>
+__device__ __forceinline__ int in_pos(int t, int q, int r) {
+  constexpr int R = Radix<N, P>::value;
+  return (t + TT * q) + r * (N / R);
+}
+
+// element position of value (q, r) of thread t at the output of pass P
+template <int N, int P, int TT>
+__device__ __forceinline__ int out_pos(int t, int q, int r) {
+  constexpr int R = Radix<N, P>::value;
+  constexpr int Ns = NsOf<N, P>::value;
+  const int j = t + TT * q;
+  const int k = j % Ns;
+  return (j - k) * R + k + r * Ns;
+}
+
+template <typename T, bool INV, int N, int P, int TT>
+__device__ __forceinline__ void compute_pass(cplx<T>* v, int t, const cplx<T>* tw) {
+  using C = cplx<T>;
+  constexpr int R = Radix<N, P>::value;
+  constexpr int Ns = NsOf<N, P>::value;
+  constexpr int Q = 8 / R;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if (Ns > 1) {
+      const int k = (t + TT * q) % Ns;
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        C w = tw[k * r * (N / (Ns * R))];
+        if (INV) w.y = -w.y;
+        v[q * R + r] = cmul(v[q * R + r], w);
+      }
+    }
+    dftR<T, INV, R>(v + q * R);
+  }
+}
+
+template <typename T, bool INV, int N, int P, int TT>
+__device__ __forceinline__ void exchange(cplx<T>* v, int t, cplx<T>* line) {
+  constexpr int R = Radix<N, P>::value, Q = 8 / R;
+  constexpr int R2 = Radix<N, P + 1>::value, Q2 = 8 / R2;
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+#pragma unroll
+    for (int r = 0; r < R; ++r) line[padpos<T>(out_pos<N, P, TT>(t, q, r))] = v[q * R + r];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q2; ++q)
+#pragma unroll
+    for (int r = 0; r < R2; ++r) v[q * R2 + r] = line[padpos<T>(in_pos<N, P + 1, TT>(t, q, r))];
+  __syncthreads();
+}
+
+template <typename T, bool INV, int N, int P, int TT>
+__device__ __forceinline__ void run_fft(cplx<T>* v, int t, const cplx<T>* tw, cplx<T>* line) {
+  compute_pass<T, INV, N, P, TT>(v, t, tw);
+  if constexpr (P + 1 < Radix<N, 0>::npass) {
+    exchange<T, INV, N, P, TT>(v, t, line);
+    run_fft<T, INV, N, P + 1, TT>(v, t, tw, line);
+  }
+}
+
+// a[i] without a runtime-indexed (local-memory) array access
+__device__ __forceinline__ int64_t pick(const int64_t* a, int i) {
+  int64_t r = a[0];
+#pragma unroll
+  for (int k = 1; k < 4; ++k)
+    if (i == k) r = a[k];
+  return r;
+}
+
+}  // namespace
+
+// B lines per CTA, N/8 threads per line.
+template <typename T, bool INV, int N, int B, bool AFAST>
+__global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) {
+  using C = cplx<T>;
+  constexpr int TT = N / 8;                  // threads per line
+  constexpr int NPASS = Radix<N, 0>::npass;
+  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16);  // padded line length
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* tile = tw + N;
+  const DevLayout ls = A.src, ld = A.dst;
+
+  int tb = blockIdx.x % A.tiles_b;
+  int rest = blockIdx.x / A.tiles_b;
+  int co0 = 0, co1 = 0;
+  if (A.o0 >= 0) {
+    co0 = rest % A.Eo0;
+    rest /= A.Eo0;
+  }
+  if (A.o1 >= 0) co1 = rest;
+  const int b0 = tb * B;
+  const int nb = min(B, A.Eb - b0);
+
+  // thread -> (line, t): lines contiguous in the warp for b-fast rows
+  int line, t;
+  if (AFAST) {
+    t = threadIdx.x % TT;
+    line = threadIdx.x / TT;
+  } else {
+    line = threadIdx.x % B;
+    t = threadIdx.x / B;
+  }
+  const bool active = line < nb;
+
+  {
+    const C* gtw = reinterpret_cast<const C*>(A.tw);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  }
+
+  // offsets shared by the whole tile (separable tables)
+  int64_t so = 0, dof = 0;
+  if (A.o0 >= 0) {
+    so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
+    dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+  }
+  if (A.o1 >= 0) {
+    so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
+    dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+  }
+
+  C v[8];
+  constexpr int R0 = Radix<N, 0>::value, Q0 = 8 / R0;
+  const C* in = reinterpret_cast<const C*>(A.in);
+  if (active) {
+    if (AFAST) {
+      const C* row = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0 + line) + __ldg(ls.t + pick(ls.off, A.a));
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r)];
+    } else {
+      const C* col = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0) + line;
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[q * R0 + r] = col[__ldg(ls.t + pick(ls.off, A.a) + in_pos<N, 0, TT>(t, q, r))];
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = mk<T>(T(0), T(0));
+  }
+  __syncthreads();  // twiddles staged
+
+  run_fft<T, INV, N, 0, TT>(v, t, tw, tile + line * LP);
+
+  constexpr int RL = Radix<N, NPASS - 1>::value, QL = 8 / RL;
+  const T s = T(A.scale);
+  C* out = reinterpret_cast<C*>(A.out);
+  if (active) {
+    if (AFAST) {
+      C* row = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0 + line) + __ldg(ld.t + pick(ld.off, A.a));
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) row[out_pos<N, NPASS - 1, TT>(t, q, r)] = cscale(v[q * RL + r], s);
+    } else {
+      C* col = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0) + line;
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r)
+          col[__ldg(ld.t + pick(ld.off, A.a) + out_pos<N, NPASS - 1, TT>(t, q, r))] = cscale(v[q * RL + r], s);
+    }
+  }
+}
+
+// Lines per CTA: at least 128-byte rows for b-fast tiles (16 complex64 or 8
+// complex128), at least 256 threads, at most 1024 threads (N/8 per line).
+template <typename T>
+constexpr int fast_lines(int n) {
+  const int rows = sizeof(T) == 4 ? 16 : 8;
+  const int want = rows > 2048 / n ? rows : 2048 / n;
+  const int cap = 8192 / n;
+  return want < cap ? want : cap;
+}
+
+template <typename T, int N, bool INV, bool AF>
+static cudaError_t launch_fast_n(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+  constexpr int B = fast_lines<T>(N);
+  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16);
+  const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
+  auto k = fft_fast_kernel<T, INV, N, B, AF>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+  }
+  k<<<tiles, N / 8 * B, smem, st>>>(A);
+  return cudaGetLastError();
+}
+
+template <typename T, int N>
+static cudaError_t launch_fast_t(const StageArgs& A, bool inverse, bool afast, unsigned tiles, cudaStream_t st) {
+  if (inverse) {
+    return afast ? launch_fast_n<T, N, true, true>(A, tiles, st) : launch_fast_n<T, N, true, false>(A, tiles, st);
+  }
+  return afast ? launch_fast_n<T, N, false, true>(A, tiles, st) : launch_fast_n<T, N, false, false>(A, tiles, st);
+}
+
+int fast_stage_lines(bool dbl, int n) { return dbl ? fast_lines<double>(n) : fast_lines<float>(n); }
+
+bool fast_stage_supported(int n) {
+  return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096;
+}
+
+cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, unsigned tiles,
+                            cudaStream_t st) {
+#define DFFT_CASE(N_)                                                                 \
+  case N_:                                                                            \
+    return dbl ? launch_fast_t<double, N_>(A, inverse, afast, tiles, st)              \
+               : launch_fast_t<float, N_>(A, inverse, afast, tiles, st);
+  switch (A.n) {
+    DFFT_CASE(16)
+    DFFT_CASE(32)
+    DFFT_CASE(64)
+    DFFT_CASE(128)
+    DFFT_CASE(256)
+    DFFT_CASE(512)
+    DFFT_CASE(1024)
+    DFFT_CASE(2048)
+    DFFT_CASE(4096)
+    default: return cudaErrorInvalidValue;
+  }
+#undef DFFT_CASE
+}
+
+}  // namespace dev
+}  // namespace dfft

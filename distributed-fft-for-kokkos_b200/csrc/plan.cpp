@@ -336,6 +336,35 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   op.smem = smem_for(B);
   op.nthreads = 256;
   if (!is_copy) A.tw = twiddle(n);
+
+  // Register-resident kernel: C2C power-of-two lines whose rows are
+  // contiguous runs on both sides (every line contiguous, or the B lines of
+  // a tile contiguous at every position along a).
+  if (kind == dev::kC2C && dev::fast_stage_supported(static_cast<int>(n)) && A.load_afast == A.store_afast &&
+      tables_[src_l].mode == 0 && tables_[dst_l].mode == 0 && S.gext[a] == n && Dl.gext[a] == n) {
+    const std::size_t Bf = static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)));
+    auto contiguous = [&](const LayoutTables& T, std::size_t axis, std::size_t len, std::size_t run) {
+      const std::int64_t* off = T.data.data() + T.off[axis];
+      for (std::size_t s0 = 0; s0 < len; s0 += run)
+        for (std::size_t c = s0 + 1; c < std::min(len, s0 + run); ++c)
+          if (off[c] != off[s0] + static_cast<std::int64_t>(c - s0)) return false;
+      return true;
+    };
+    bool ok;
+    if (A.load_afast) {
+      ok = contiguous(tables_[src_l], a, n, n) && contiguous(tables_[dst_l], a, n, n);
+    } else {
+      ok = contiguous(tables_[src_l], b, Dl.gext[b], Bf) && contiguous(tables_[dst_l], b, Dl.gext[b], Bf);
+    }
+    if (ok) {
+      op.fast = true;
+      A.B = static_cast<int>(Bf);
+      A.tiles_b = static_cast<int>((Dl.gext[b] + Bf - 1) / Bf);
+      const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
+      if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
+      op.tiles = static_cast<unsigned>(ft);
+    }
+  }
   return op;
 }
 
@@ -709,7 +738,10 @@ void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream)
         dev::StageArgs A = op0.sa;
         A.in = buf(op0.src);
         A.out = buf(op0.dst);
-        e = dev::launch_fft_stage(A, d_.dbl, op0.kind, op0.inverse, op0.nthreads, op0.smem, op0.tiles, stream);
+        if (op0.fast)
+          e = dev::launch_fft_fast(A, d_.dbl, op0.inverse, A.load_afast != 0, op0.tiles, stream);
+        else
+          e = dev::launch_fft_stage(A, d_.dbl, op0.kind, op0.inverse, op0.nthreads, op0.smem, op0.tiles, stream);
         break;
       }
       case Op::Pack:

@@ -37,6 +37,7 @@ struct Op {
   dev::StageArgs sa{};
   int kind = 0;
   bool inverse = false;
+  bool fast = false;  // register-resident power-of-two kernel
   int nthreads = 256;
   std::size_t smem = 0;
   unsigned tiles = 0;

@@ -212,3 +212,13 @@ def test_input_not_modified_and_errors():
         dfft.execute(plan, t_in, t_in, dfft.Direction.forward)
     with pytest.raises(ValueError):
         dfft.execute(plan, t_in, t_out, 7)
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 1024, 2048, 4096])
+def test_register_kernel_line_lengths(n, precision):
+    # lines along the unit-stride axis (a-fast rows) and across it (b-fast rows),
+    # on a slab exchange so the rows also cross virtual-rank blocks
+    for gin, axes, tin, tout in [((4, 6, n), (2,), (2, 1, 1), (1, 2, 1)), ((n, 3, 32), (0,), (1, 1, 2), (1, 1, 2)),
+                                 ((n, 3, 32), (0,), (1, 2, 1), (1, 1, 2))]:
+        check_roundtrip(gin, axes, tin, tout, False, precision=precision)

@@ -311,6 +311,23 @@ dfft_status dfft_get_all_topologies(int32_t pencil, int32_t rank, const uint64_t
   });
 }
 
+}  // extern "C"
+
+dfft_status dfft_noalloc_impl(const void* in, void* out, int64_t n0, int64_t n1, int64_t n2, int32_t precision,
+                              int32_t direction, int32_t normalization, void* stream, const char** err);
+
+extern "C" {
+
+dfft_status dfft_execute_local_c2c_noalloc(const void* in, void* out, int64_t n0, int64_t n1, int64_t n2,
+                                           int32_t precision, int32_t direction, int32_t normalization,
+                                           void* stream) {
+  const char* err = "";
+  const dfft_status st = dfft_noalloc_impl(in, out, n0, n1, n2, precision, direction, normalization, stream, &err);
+  if (st != DFFT_SUCCESS) return set_error(st, err);
+  g_last_error.clear();
+  return DFFT_SUCCESS;
+}
+
 const char* dfft_last_error_string(void) { return g_last_error.c_str(); }
 
 const char* dfft_version(void) { return "dfft-b200 0.1.0"; }

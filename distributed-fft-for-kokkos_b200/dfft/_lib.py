@@ -86,6 +86,9 @@ SIGNATURES = {
                        ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64),
                        ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int64),
                        ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_execute_local_c2c_noalloc": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     "dfft_last_error_string": (ctypes.c_char_p, []),
     "dfft_version": (ctypes.c_char_p, []),
 }

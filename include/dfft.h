@@ -198,6 +198,30 @@ dfft_status dfft_get_launch_count(const dfft_plan* plan, int32_t direction, int6
 /* Bytes of device memory the plan holds (scratch, tables, debug buffers). */
 dfft_status dfft_get_workspace_bytes(const dfft_plan* plan, uint64_t* bytes);
 
+/* Local 3D C2C FFT that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: programs whose device
+ * memory is already owned by another allocator (for example a framework's
+ * caching pool that reserved the GPU up front), and latency-critical loops
+ * that must not hit cudaMalloc / cudaFree, which can synchronise the device.
+ *
+ * Transforms all three axes of one C-order array of n0 x n1 x n2 complex
+ * elements (complex128 for DFFT_PREC_F64, complex64 for DFFT_PREC_F32), the
+ * local transform each rank of the reference runs; in / out are device
+ * pointers to distinct arrays and `stream` is a cudaStream_t (NULL: legacy
+ * default stream).  The intermediate array between the axis stages lives in a
+ * library-owned __device__ array of DFFT_NOALLOC_MAX_BYTES, which every GPU
+ * that loads the library holds until the process exits.
+ *   - every extent must be a power of two in [16, 4096] and the array at most
+ *     DFFT_NOALLOC_MAX_BYTES; otherwise DFFT_ERROR_UNSUPPORTED;
+ *   - the first call on a device sets the device up (synchronous copies of
+ *     the twiddle tables): make it before any stream capture;
+ *   - all calls share the library-owned arrays: calls that overlap on the GPU
+ *     race with each other. */
+#define DFFT_NOALLOC_MAX_BYTES (64ull * 1024ull * 1024ull)
+dfft_status dfft_execute_local_c2c_noalloc(const void* in, void* out, int64_t n0, int64_t n1, int64_t n2,
+                                           int32_t precision, int32_t direction, int32_t normalization,
+                                           void* stream);
+
 /* Message of the last failure on this thread ("" if none). */
 const char* dfft_last_error_string(void);
 

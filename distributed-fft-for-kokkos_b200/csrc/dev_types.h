@@ -66,6 +66,8 @@ cudaError_t launch_fft_stage(const StageArgs& A, bool dbl, int kind, bool invers
 // C2C, rows contiguous on both sides.
 bool fast_stage_supported(int n);
 int fast_stage_lines(bool dbl, int n);
+// Lines-per-CTA variants the launcher accepts (A.B must be one of them).
+int fast_stage_line_options(bool dbl, int n, int* opts);
 cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, unsigned tiles,
                             cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack

@@ -187,7 +187,10 @@ __global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) 
   using C = cplx<T>;
   constexpr int TT = N / 8;                  // threads per line
   constexpr int NPASS = Radix<N, 0>::npass;
-  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16);  // padded line length
+  // padded line length: one pad per 256 bytes inside a line, and an odd
+  // 8-byte (complex64) / 16-byte (complex128) stride between lines so that
+  // the lines of a b-fast warp fall in different banks
+  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16) + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* tile = tw + N;
@@ -277,8 +280,9 @@ __global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) 
   }
 }
 
-// Lines per CTA: at least 128-byte rows for b-fast tiles (16 complex64 or 8
-// complex128), at least 256 threads, at most 1024 threads (N/8 per line).
+// Default lines per CTA: at least 128-byte rows for b-fast tiles (16
+// complex64 or 8 complex128), at least 256 threads, at most 1024 threads
+// (N/8 per line).  The launcher also has variants with 1/2 and 1/4 of it.
 template <typename T>
 constexpr int fast_lines(int n) {
   const int rows = sizeof(T) == 4 ? 16 : 8;
@@ -287,10 +291,9 @@ constexpr int fast_lines(int n) {
   return want < cap ? want : cap;
 }
 
-template <typename T, int N, bool INV, bool AF>
-static cudaError_t launch_fast_n(const StageArgs& A, unsigned tiles, cudaStream_t st) {
-  constexpr int B = fast_lines<T>(N);
-  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16);
+template <typename T, int N, bool INV, bool AF, int B>
+static cudaError_t launch_fast_b(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16) + 1;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
   auto k = fft_fast_kernel<T, INV, N, B, AF>;
   if (smem > 48 * 1024) {
@@ -299,6 +302,17 @@ static cudaError_t launch_fast_n(const StageArgs& A, unsigned tiles, cudaStream_
   }
   k<<<tiles, N / 8 * B, smem, st>>>(A);
   return cudaGetLastError();
+}
+
+template <typename T, int N, bool INV, bool AF>
+static cudaError_t launch_fast_n(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+  constexpr int B0 = fast_lines<T>(N);
+  constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
+  constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
+  if (A.B == B0) return launch_fast_b<T, N, INV, AF, B0>(A, tiles, st);
+  if (A.B == B1) return launch_fast_b<T, N, INV, AF, B1>(A, tiles, st);
+  if (A.B == B2) return launch_fast_b<T, N, INV, AF, B2>(A, tiles, st);
+  return cudaErrorInvalidValue;
 }
 
 template <typename T, int N>
@@ -310,6 +324,15 @@ static cudaError_t launch_fast_t(const StageArgs& A, bool inverse, bool afast, u
 }
 
 int fast_stage_lines(bool dbl, int n) { return dbl ? fast_lines<double>(n) : fast_lines<float>(n); }
+
+int fast_stage_line_options(bool dbl, int n, int* opts) {
+  const int b0 = fast_stage_lines(dbl, n);
+  int k = 0;
+  opts[k++] = b0;
+  if (b0 / 2 >= 1 && b0 / 2 != b0) opts[k++] = b0 / 2;
+  if (b0 / 4 >= 1 && b0 / 4 != b0 / 2) opts[k++] = b0 / 4;
+  return k;
+}
 
 bool fast_stage_supported(int n) {
   return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096;

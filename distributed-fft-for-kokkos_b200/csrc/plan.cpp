@@ -21,6 +21,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <fstream>
+#include <limits>
+#include <mutex>
+#include <sstream>
 #include <cstring>
 
 namespace dfft {
@@ -84,6 +89,7 @@ Plan::Plan(const PlanDesc& d, bool on_device) : d_(d), on_device_(on_device) {
       build_literal(false);
     }
     allocate_device();
+    autotune();
   } catch (...) {
     for (auto p : bufs_)
       if (p) cudaFree(p);
@@ -714,6 +720,106 @@ void Plan::allocate_device() {
         if (op.type == Op::Pack) op.xa.lay = dev_layout(op.src_layout);
         if (op.type == Op::Unpack) op.xa.lay = dev_layout(op.dst_layout);
       }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: lines per CTA of every register-resident stage, timed on the
+// plan's scratch buffers at plan creation and cached per stage signature
+// (line length, precision, direction, row orientation, tile grid) for the
+// process; DFFT_TUNE_CACHE=<file> also persists the choices across processes
+// and DFFT_AUTOTUNE=0 keeps the defaults.
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::string, int> g_tune_cache;
+bool g_tune_loaded = false;
+
+void load_tune_cache_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* path = std::getenv("DFFT_TUNE_CACHE");
+  if (!path) return;
+  std::ifstream f(path);
+  std::string key;
+  int val;
+  while (f >> key >> val) g_tune_cache[key] = val;
+}
+
+void store_tune_locked(const std::string& key, int val) {
+  g_tune_cache[key] = val;
+  const char* path = std::getenv("DFFT_TUNE_CACHE");
+  if (!path) return;
+  std::ofstream f(path, std::ios::app);
+  f << key << " " << val << "\n";
+}
+}  // namespace
+
+void Plan::autotune() {
+  const char* env = std::getenv("DFFT_AUTOTUNE");
+  if (env && std::string(env) == "0") return;
+  if (bufs_.size() <= kBufScratch1 || !bufs_[kBufScratch0] || !bufs_[kBufScratch1]) return;
+  cudaStream_t st = d_.stream;
+  void* s0 = bufs_[kBufScratch0];
+  void* s1 = bufs_[kBufScratch1];
+  bool cleared = false;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  load_tune_cache_locked();
+  for (auto& prog : prog_) {
+    for (auto& op : prog) {
+      if (op.type != Op::Stage || !op.fast) continue;
+      dev::StageArgs& A = op.sa;
+      std::ostringstream k;
+      k << "fast:n" << A.n << (d_.dbl ? "f64" : "f32") << (op.inverse ? "i" : "f") << (A.load_afast ? "a" : "b")
+        << ":" << A.Eb << "x" << A.Eo0 << "x" << A.Eo1;
+      const std::string key = k.str();
+      auto apply = [&](int B) {
+        A.B = B;
+        A.tiles_b = (A.Eb + B - 1) / B;
+        op.tiles = static_cast<unsigned>(static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1);
+      };
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        apply(it->second);
+        continue;
+      }
+      if (!cleared) {
+        cuda_check(cudaMemsetAsync(s0, 0, buf_bytes_[kBufScratch0], st), "tuner clear");
+        cuda_check(cudaMemsetAsync(s1, 0, buf_bytes_[kBufScratch1], st), "tuner clear");
+        cleared = true;
+      }
+      int opts[4];
+      const int nopt = dev::fast_stage_line_options(d_.dbl, A.n, opts);
+      int best = A.B;
+      float best_ms = std::numeric_limits<float>::max();
+      cudaEvent_t e0, e1;
+      cuda_check(cudaEventCreate(&e0), "tuner event");
+      cuda_check(cudaEventCreate(&e1), "tuner event");
+      for (int i = 0; i < nopt; ++i) {
+        apply(opts[i]);
+        dev::StageArgs T = A;
+        T.in = s0;
+        T.out = s1;
+        if (dev::launch_fft_fast(T, d_.dbl, op.inverse, A.load_afast != 0, op.tiles, st) != cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3; ++r) dev::launch_fft_fast(T, d_.dbl, op.inverse, A.load_afast != 0, op.tiles, st);
+        cudaEventRecord(e1, st);
+        cuda_check(cudaEventSynchronize(e1), "tuner sync");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = opts[i];
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      apply(best);
+      store_tune_locked(key, best);
     }
   }
 }

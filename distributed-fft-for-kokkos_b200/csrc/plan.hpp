@@ -115,6 +115,7 @@ class Plan {
   void finalize_program(std::vector<Op>& prog, int cur_layout, int cur_buf, const Layout& final_layout,
                         double scale, bool final_complex);
   void allocate_device();
+  void autotune();
   const void* twiddle(std::size_t n);
 };
 

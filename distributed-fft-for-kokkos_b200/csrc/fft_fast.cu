@@ -101,10 +101,25 @@ struct NsOf<N, 0> {
   static constexpr int value = 1;
 };
 
-// padded shared-memory position: one pad element per 256 bytes
-template <typename T>
+// Shared-memory layout of a line: position p is stored at p + (p >> S) and
+// lines are LP elements apart.  S and the pitch offset were chosen by an
+// offline model of the bank wavefronts of every exchange of every plan and
+// thread mapping (one pad per 8 elements, or per 16 for complex64 lines of
+// 128+ points read along the line), which keeps the exchanges within ~1.1x of
+// conflict-free.
+template <typename T, int N, int B, bool AFAST>
+struct SmemShape {
+  static constexpr bool f32 = sizeof(T) == 4;
+  static constexpr int S = (f32 && ((AFAST && N >= 128) || (!AFAST && B == 1))) ? 4 : 3;
+  static constexpr int extra_afast = (N <= (f32 ? 64 : 32)) ? 1 : 0;
+  static constexpr int full = f32 ? 16 : 8;
+  static constexpr int extra_bfast = (B >= full) ? 0 : (B * 2 == full) ? 3 : (B * 4 == full) ? 5 : (B * 8 == full) ? 9 : 0;
+  static constexpr int LP = (N - 1) + ((N - 1) >> S) + 1 + (AFAST ? extra_afast : extra_bfast);
+};
+
+template <int S>
 __device__ __forceinline__ int padpos(int p) {
-  return sizeof(T) == 4 ? p + (p >> 5) : p + (p >> 4);
+  return p + (p >> S);
 }
 
 // element position of value (q, r) of thread t at the input of pass P
@@ -134,39 +149,59 @@ __device__ __forceinline__ void compute_pass(cplx<T>* v, int t, const cplx<T>* t
   for (int q = 0; q < Q; ++q) {
     if (Ns > 1) {
       const int k = (t + TT * q) % Ns;
+      const int m = k * (N / (Ns * R));  // w = tw[m] = exp(-2 pi i k / (Ns R))
+      if constexpr (R == 8) {
+        // three table reads (w, w^2, w^4); the other powers are products of
+        // at most two of them
+        C w1 = tw[m], w2 = tw[2 * m], w4 = tw[4 * m];
+        if (INV) {
+          w1.y = -w1.y;
+          w2.y = -w2.y;
+          w4.y = -w4.y;
+        }
+        const C w3 = cmul(w1, w2);
+        v[q * R + 1] = cmul(v[q * R + 1], w1);
+        v[q * R + 2] = cmul(v[q * R + 2], w2);
+        v[q * R + 3] = cmul(v[q * R + 3], w3);
+        v[q * R + 4] = cmul(v[q * R + 4], w4);
+        v[q * R + 5] = cmul(v[q * R + 5], cmul(w1, w4));
+        v[q * R + 6] = cmul(v[q * R + 6], cmul(w2, w4));
+        v[q * R + 7] = cmul(v[q * R + 7], cmul(w3, w4));
+      } else {
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        C w = tw[k * r * (N / (Ns * R))];
-        if (INV) w.y = -w.y;
-        v[q * R + r] = cmul(v[q * R + r], w);
+        for (int r = 1; r < R; ++r) {
+          C w = tw[r * m];
+          if (INV) w.y = -w.y;
+          v[q * R + r] = cmul(v[q * R + r], w);
+        }
       }
     }
     dftR<T, INV, R>(v + q * R);
   }
 }
 
-template <typename T, bool INV, int N, int P, int TT>
+template <typename T, bool INV, int N, int P, int TT, int S>
 __device__ __forceinline__ void exchange(cplx<T>* v, int t, cplx<T>* line) {
   constexpr int R = Radix<N, P>::value, Q = 8 / R;
   constexpr int R2 = Radix<N, P + 1>::value, Q2 = 8 / R2;
 #pragma unroll
   for (int q = 0; q < Q; ++q)
 #pragma unroll
-    for (int r = 0; r < R; ++r) line[padpos<T>(out_pos<N, P, TT>(t, q, r))] = v[q * R + r];
+    for (int r = 0; r < R; ++r) line[padpos<S>(out_pos<N, P, TT>(t, q, r))] = v[q * R + r];
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < Q2; ++q)
 #pragma unroll
-    for (int r = 0; r < R2; ++r) v[q * R2 + r] = line[padpos<T>(in_pos<N, P + 1, TT>(t, q, r))];
+    for (int r = 0; r < R2; ++r) v[q * R2 + r] = line[padpos<S>(in_pos<N, P + 1, TT>(t, q, r))];
   __syncthreads();
 }
 
-template <typename T, bool INV, int N, int P, int TT>
+template <typename T, bool INV, int N, int P, int TT, int S>
 __device__ __forceinline__ void run_fft(cplx<T>* v, int t, const cplx<T>* tw, cplx<T>* line) {
   compute_pass<T, INV, N, P, TT>(v, t, tw);
   if constexpr (P + 1 < Radix<N, 0>::npass) {
-    exchange<T, INV, N, P, TT>(v, t, line);
-    run_fft<T, INV, N, P + 1, TT>(v, t, tw, line);
+    exchange<T, INV, N, P, TT, S>(v, t, line);
+    run_fft<T, INV, N, P + 1, TT, S>(v, t, tw, line);
   }
 }
 
@@ -187,10 +222,8 @@ __global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) 
   using C = cplx<T>;
   constexpr int TT = N / 8;                  // threads per line
   constexpr int NPASS = Radix<N, 0>::npass;
-  // padded line length: one pad per 256 bytes inside a line, and an odd
-  // 8-byte (complex64) / 16-byte (complex128) stride between lines so that
-  // the lines of a b-fast warp fall in different banks
-  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16) + 1;
+  using SH = SmemShape<T, N, B, AFAST>;
+  constexpr int LP = SH::LP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* tile = tw + N;
@@ -257,7 +290,7 @@ __global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) 
   }
   __syncthreads();  // twiddles staged
 
-  run_fft<T, INV, N, 0, TT>(v, t, tw, tile + line * LP);
+  run_fft<T, INV, N, 0, TT, SH::S>(v, t, tw, tile + line * LP);
 
   constexpr int RL = Radix<N, NPASS - 1>::value, QL = 8 / RL;
   const T s = T(A.scale);
@@ -293,7 +326,7 @@ constexpr int fast_lines(int n) {
 
 template <typename T, int N, bool INV, bool AF, int B>
 static cudaError_t launch_fast_b(const StageArgs& A, unsigned tiles, cudaStream_t st) {
-  constexpr int LP = N + N / (sizeof(T) == 4 ? 32 : 16) + 1;
+  constexpr int LP = SmemShape<T, N, B, AF>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
   auto k = fft_fast_kernel<T, INV, N, B, AF>;
   if (smem > 48 * 1024) {

@@ -96,15 +96,18 @@ def test_lower_rank_fft_plans(exec_mode):
     check_roundtrip((8, 7, 5), (0, 2), (1, 2, 2), (2, 2, 1), True, exec_mode=exec_mode)
 
 
-def test_fused_equals_literal_c2c_bitwise():
-    # C2C: the fused path and the reference block sequence run the same per-line
-    # arithmetic, so their results agree bit for bit
+def test_fused_equals_literal_c2c():
+    # The fused path and the reference block sequence agree to FP64 rounding.
+    # They are not bit-identical: a stage may run on the register-resident
+    # kernel in one path and on the generic Stockham kernel in the other (the
+    # choice depends on the layouts), and those derive their twiddles
+    # differently.  The exchanges themselves are checked bit for bit below.
     gin = (32, 24, 20)
     x = random_input(gin, False, 5)
     pf = dfft.Plan(gin, gin, (0, 1, 2), (4, 2, 1), (1, 4, 2), exec_mode="fused")
     pl = dfft.Plan(gin, gin, (0, 1, 2), (4, 2, 1), (1, 4, 2), exec_mode="literal")
     a, b = run(pf, x, True), run(pl, x, True)
-    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    assert O.rel_l2(a, b) <= 1e-14
 
 
 def _bitwise_equal(a, b):

@@ -70,7 +70,7 @@ def start_clock_sampler(device):
          "clocks_event_reasons.sw_power_cap")
     try:
         p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                              "-lms", "200"], stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+                              "-lms", "100"], stdout=open(path, "w"), stderr=subprocess.DEVNULL)
     except Exception:
         p = None
     return p, path
@@ -164,10 +164,12 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="run only the FP32 warm-up and timed steps (for ncu captures); prints no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -233,6 +235,9 @@ def main():
     ms32 = max_over_ranks(timed(p32, a32, b32, c32, args.steps))
     clocks = stop_clock_sampler(*sampler)
     launches = p32.launch_count(dfft.Direction.forward) + p32.launch_count(dfft.Direction.backward)
+    if args.profile:
+        print(f"profile run: {ms32:.4f} ms per step (not a bench value)", flush=True)
+        return
 
     # ---- plain FP64 path and the error of the FP32 result ----
     p64 = make("float64")
@@ -275,10 +280,12 @@ def main():
     per_launch_bytes = step_bytes / launches
     launch_ms = ms32 / launches
     achieved = per_launch_bytes / (launch_ms * 1e-3) / 1e9
-    traffic = None
+    traffic = None  # dram bytes per launch from the committed full ncu capture of this workload
     try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            traffic = json.load(f).get("fft_stage_512_c64_per_launch_bytes")
+        with open(os.path.join(ROOT, "profiles", "fft_fast_kernel_512cubed_c64_full.md")) as f:
+            for ln in f:
+                if ln.startswith("traffic_per_launch_bytes:"):
+                    traffic = int(ln.split(":")[1])
     except Exception:
         pass
 
@@ -299,7 +306,7 @@ def main():
             "e2e": {"value": round(world * step_bytes / (ms_e2e * 1e-3) / 1e9, 2), "unit": "GB/s",
                     "ms_per_step": round(ms_e2e, 3), "h2d_bytes_per_step": int(h_in.numel() * 8),
                     "d2h_bytes_per_step": int(h_out.numel() * 8)},
-            "roofline": {"bound": "hbm", "kernel": "fft_stage_kernel (every launch of the step)",
+            "roofline": {"bound": "hbm", "kernel": "fft_fast_kernel (every launch of the step: 3 axis stages per direction)",
                          "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "algorithmic_bytes_per_launch": int(per_launch_bytes)},

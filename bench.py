@@ -226,13 +226,28 @@ def main():
         return e0.elapsed_time(e1) / steps
 
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
-    # ---- FP32 fused path (headline) ----
+    # ---- FP32 fused path (headline): fwd + bwd captured in one CUDA graph ----
     p32 = make("float32")
     a32 = torch.randn(n ** 3, dtype=torch.complex64, device="cuda", generator=gen)
     b32 = torch.empty_like(a32)
     c32 = torch.empty_like(a32)
+    ms32_eager = max_over_ranks(timed(p32, a32, b32, c32, max(3, args.steps // 4)))
+    graph = dfft.Graph([(p32, a32, b32, dfft.Direction.forward, 0), (p32, b32, c32, dfft.Direction.backward, 0)])
+
+    def timed_graph(steps):
+        for _ in range(args.warmup):
+            graph.launch(stream.cuda_stream)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            graph.launch(stream.cuda_stream)
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
     sampler = start_clock_sampler(local)
-    ms32 = max_over_ranks(timed(p32, a32, b32, c32, args.steps))
+    ms32 = max_over_ranks(timed_graph(args.steps))
     clocks = stop_clock_sampler(*sampler)
     launches = p32.launch_count(dfft.Direction.forward) + p32.launch_count(dfft.Direction.backward)
     if args.profile:
@@ -251,6 +266,54 @@ def main():
     err_fwd = float(torch.linalg.vector_norm(b32.to(torch.complex128) - b64) / torch.linalg.vector_norm(b64))
     err_rt = float(torch.linalg.vector_norm(c32.to(torch.complex128) - a64) / torch.linalg.vector_norm(a64))
     del a64, b64, c64, p64
+    torch.cuda.empty_cache()
+
+    # ---- 16 uneven fields (edges from {64,96,128,192}, rng seed 2): FP32 graph
+    # of all fields (concurrent branches) vs the plain FP64 per-field loop ----
+    import numpy as np
+    edges = np.random.default_rng(2).choice([64, 96, 128, 192], size=16)
+    batch = {}
+    for prec in ("float32", "float64"):
+        dt = torch.complex64 if prec == "float32" else torch.complex128
+        fields = []
+        for e in edges:
+            e = int(e)
+            pl = dfft.Plan((e,) * 3, (e,) * 3, (0, 1, 2), (2, 2, 1), (1, 2, 2), precision=prec,
+                           stream=stream.cuda_stream)
+            x = torch.randn(e ** 3, dtype=dt, device="cuda", generator=gen)
+            fields.append((pl, x, torch.empty_like(x), torch.empty_like(x)))
+        batch[prec] = fields
+    items = []
+    for i, (pl, x, y, z) in enumerate(batch["float32"]):
+        items += [(pl, x, y, dfft.Direction.forward, i), (pl, y, z, dfft.Direction.backward, i)]
+    bgraph = dfft.Graph(items)
+    bsteps = max(3, args.steps // 10)
+    for _ in range(args.warmup):
+        bgraph.launch(stream.cuda_stream)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(bsteps):
+        bgraph.launch(stream.cuda_stream)
+    e1.record(stream)
+    barrier()
+    ms_batch32 = max_over_ranks(e0.elapsed_time(e1) / bsteps)
+
+    def loop64():
+        for pl, x, y, z in batch["float64"]:
+            dfft.execute(pl, x, y, dfft.Direction.forward)
+            dfft.execute(pl, y, z, dfft.Direction.backward)
+    for _ in range(args.warmup):
+        loop64()
+    barrier()
+    e0.record(stream)
+    for _ in range(bsteps):
+        loop64()
+    e1.record(stream)
+    barrier()
+    ms_batch64 = max_over_ranks(e0.elapsed_time(e1) / bsteps)
+    batch_bytes = sum(algo_bytes(int(e), 8) for e in edges)
+    del batch, bgraph, items
     torch.cuda.empty_cache()
 
     # ---- end to end through the C ABI with host buffers ----
@@ -295,10 +358,16 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(ms32, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (complex N(0,1), torch generator seed 1234+rank)",
             "config": {"workload": WORKLOAD, "n": n, "topology_in": list(TOPO_IN), "topology_out": list(TOPO_OUT),
-                       "precision": "complex64", "exec_mode": "fused",
+                       "precision": "complex64", "exec_mode": "fused", "graph": True,
                        "l2": "inputs (1 GiB per field) larger than the 126 MB L2",
                        "parallelism": f"weak, one 512^3 field per GPU x {world}"},
             "gflops": round(world * flops(n) / (ms32 * 1e-3) / 1e9, 1),
+            "execution": "CUDA graph of forward + backward (plan-time autotuned kernels)",
+            "eager_ms_per_step": round(ms32_eager, 4),
+            "batch16_uneven": {"edges": [int(e) for e in edges], "fp32_graph_ms": round(ms_batch32, 4),
+                               "fp64_loop_ms": round(ms_batch64, 4),
+                               "speedup": round(ms_batch64 / ms_batch32, 3),
+                               "fp32_graph_GBps": round(batch_bytes / (ms_batch32 * 1e-3) / 1e9, 1)},
             "fp64_ms_per_step": round(ms64, 4),
             "fp32_over_fp64_speedup": round(ms64 / ms32, 3),
             "rel_l2_fp32_vs_fp64_forward": err_fwd,

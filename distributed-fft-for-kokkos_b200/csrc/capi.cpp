@@ -2,15 +2,22 @@
 // the planner's exceptions and turns them into a dfft_status plus a
 // thread-local message (the reference throws std::runtime_error via
 // KOKKOSFFT_THROW_IF; nothing may unwind across a C ABI).
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/dfft.h"
 #include "plan.hpp"
 
 struct dfft_plan_s {
   dfft::Plan* impl;
+};
+
+struct dfft_graph_s {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
 
 namespace {
@@ -326,6 +333,106 @@ dfft_status dfft_execute_local_c2c_noalloc(const void* in, void* out, int64_t n0
   if (st != DFFT_SUCCESS) return set_error(st, err);
   g_last_error.clear();
   return DFFT_SUCCESS;
+}
+
+dfft_status dfft_graph_create(dfft_graph** graph, const dfft_plan* const* plans, const void* const* ins,
+                              void* const* outs, const int32_t* directions, const int32_t* branch_ids,
+                              int64_t count) {
+  return guarded([&] {
+    if (!graph || !plans || !ins || !outs || !directions || count <= 0)
+      dfft::fail(dfft::kErrInvalidArgument, "null argument or empty batch");
+    *graph = nullptr;
+    for (int64_t i = 0; i < count; ++i) {
+      impl_of(plans[i]);
+      if (directions[i] != DFFT_FORWARD && directions[i] != DFFT_BACKWARD)
+        dfft::fail(dfft::kErrInvalidArgument, "Invalid FFT direction specified.");
+    }
+    auto ck = [](cudaError_t e, const char* what) {
+      if (e != cudaSuccess) dfft::fail(dfft::kErrCuda, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    // branch of every item: its id in branch_ids, or its own
+    std::vector<int> bidx(static_cast<std::size_t>(count));
+    std::vector<int32_t> ids;
+    for (int64_t i = 0; i < count; ++i) {
+      const int32_t id = branch_ids ? branch_ids[i] : static_cast<int32_t>(i);
+      auto it = std::find(ids.begin(), ids.end(), id);
+      if (it == ids.end()) {
+        bidx[i] = static_cast<int>(ids.size());
+        ids.push_back(id);
+      } else {
+        bidx[i] = static_cast<int>(it - ids.begin());
+      }
+    }
+    const std::size_t nb = ids.size();
+    cudaStream_t cap = nullptr;
+    ck(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream create");
+    std::vector<cudaStream_t> branches(nb, nullptr);
+    std::vector<cudaEvent_t> done(nb, nullptr);
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t g = nullptr;
+    auto cleanup = [&]() {
+      for (auto s2 : branches)
+        if (s2) cudaStreamDestroy(s2);
+      for (auto e : done)
+        if (e) cudaEventDestroy(e);
+      if (fork) cudaEventDestroy(fork);
+      if (cap) cudaStreamDestroy(cap);
+    };
+    try {
+      ck(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event create");
+      for (std::size_t b = 0; b < nb; ++b) {
+        ck(cudaStreamCreateWithFlags(&branches[b], cudaStreamNonBlocking), "stream create");
+        ck(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming), "event create");
+      }
+      ck(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+      try {
+        ck(cudaEventRecord(fork, cap), "fork record");
+        for (std::size_t b = 0; b < nb; ++b) ck(cudaStreamWaitEvent(branches[b], fork, 0), "fork wait");
+        for (int64_t i = 0; i < count; ++i)
+          plans[i]->impl->execute(ins[i], outs[i], directions[i] == DFFT_FORWARD, branches[bidx[i]]);
+        for (std::size_t b = 0; b < nb; ++b) {
+          ck(cudaEventRecord(done[b], branches[b]), "join record");
+          ck(cudaStreamWaitEvent(cap, done[b], 0), "join wait");
+        }
+      } catch (...) {
+        cudaGraph_t dead = nullptr;
+        cudaStreamEndCapture(cap, &dead);
+        if (dead) cudaGraphDestroy(dead);
+        throw;
+      }
+      ck(cudaStreamEndCapture(cap, &g), "end capture");
+      auto* out = new dfft_graph_s;
+      out->graph = g;
+      if (cudaGraphInstantiate(&out->exec, g, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        delete out;
+        dfft::fail(dfft::kErrCuda, "cudaGraphInstantiate failed");
+      }
+      *graph = out;
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
+  });
+}
+
+dfft_status dfft_graph_launch(const dfft_graph* graph, void* stream) {
+  return guarded([&] {
+    if (!graph || !graph->exec) dfft::fail(dfft::kErrInvalidArgument, "null graph");
+    const cudaError_t e = cudaGraphLaunch(graph->exec, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) dfft::fail(dfft::kErrCuda, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+  });
+}
+
+dfft_status dfft_graph_destroy(dfft_graph* graph) {
+  return guarded([&] {
+    if (!graph) return;
+    if (graph->exec) cudaGraphExecDestroy(graph->exec);
+    if (graph->graph) cudaGraphDestroy(graph->graph);
+    delete graph;
+  });
 }
 
 const char* dfft_last_error_string(void) { return g_last_error.c_str(); }

@@ -329,9 +329,12 @@ static cudaError_t launch_fast_b(const StageArgs& A, unsigned tiles, cudaStream_
   constexpr int LP = SmemShape<T, N, B, AF>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
   auto k = fft_fast_kernel<T, INV, N, B, AF>;
-  if (smem > 48 * 1024) {
+  // raise the dynamic shared-memory limit once per kernel (not inside graph captures)
+  static size_t attr_bytes = 48 * 1024;
+  if (smem > attr_bytes) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
+    attr_bytes = smem;
   }
   k<<<tiles, N / 8 * B, smem, st>>>(A);
   return cudaGetLastError();

@@ -366,9 +366,13 @@ static cudaError_t launch_stage_t(const StageArgs& A, int kind, bool inverse, in
     case kCopyReal: k = fft_stage_kernel<T, kCopyReal, false>; break;
     default: return cudaErrorInvalidValue;
   }
-  if (smem > 48 * 1024) {
+  // raise the dynamic shared-memory limit once per kernel (not inside graph captures)
+  static size_t attr_bytes[2 * 5] = {};
+  size_t& done = attr_bytes[kind * 2 + (inverse ? 1 : 0)];
+  if (smem > 48 * 1024 && smem > done) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
+    done = smem;
   }
   k<<<tiles, nthreads, smem, st>>>(A);
   return cudaGetLastError();

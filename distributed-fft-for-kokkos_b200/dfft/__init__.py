@@ -7,6 +7,7 @@ from .plan import (  # noqa: F401
     Direction,
     DistributedFFTError,
     ExecMode,
+    Graph,
     Normalization,
     Plan,
     Status,

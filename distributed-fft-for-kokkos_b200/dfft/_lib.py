@@ -89,6 +89,12 @@ SIGNATURES = {
     "dfft_execute_local_c2c_noalloc": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                        ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    "dfft_graph_create": (
+        ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                       ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                       ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.c_int64]),
+    "dfft_graph_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dfft_last_error_string": (ctypes.c_char_p, []),
     "dfft_version": (ctypes.c_char_p, []),
 }

@@ -260,6 +260,33 @@ class Plan:
         return out
 
 
+class Graph:
+    """A CUDA graph holding a batch of transforms: ``items`` is a list of
+    (plan, in_buf, out_buf, direction[, branch]); items with the same branch
+    run in order, different branches run concurrently (default: one branch per
+    item).  Every ``launch()`` replays them on the same buffers."""
+
+    def __init__(self, items):
+        n = len(items)
+        br = (ctypes.c_int32 * n)(*[int(it[4]) if len(it) > 4 else i for i, it in enumerate(items)])
+        plans = (ctypes.c_void_p * n)(*[it[0]._h.value for it in items])
+        ins = (ctypes.c_void_p * n)(*[_ptr(it[1]).value for it in items])
+        outs = (ctypes.c_void_p * n)(*[_ptr(it[2]).value for it in items])
+        dirs = (ctypes.c_int32 * n)(*[int(Direction(it[3])) for it in items])
+        self._keep = [it[0] for it in items]  # plans must outlive the graph
+        self._h = ctypes.c_void_p()
+        _check(lib.dfft_graph_create(ctypes.byref(self._h), plans, ins, outs, dirs, br, n))
+
+    def launch(self, stream=None):
+        _check(lib.dfft_graph_launch(self._h, ctypes.c_void_p(int(stream)) if stream else None))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dfft_graph_destroy(h)
+            self._h = None
+
+
 def all_topologies(kind, in_topology, out_topology, axes, in_layout="right", out_layout="right"):
     """get_all_slab_topologies / get_all_pencil_topologies on their own.
 

@@ -172,6 +172,21 @@ dfft_status dfft_get_max_buffer_size(const dfft_plan* plan, uint64_t* size);
 dfft_status dfft_get_topology_chain(const dfft_plan* plan, int64_t* n, uint64_t* topologies, int64_t* trans_axes,
                                     int64_t* layouts);
 
+/* ---- Batched execution under a CUDA graph ----
+ * Captures, once, the execution of `count` transforms (plans[i] applied to
+ * ins[i] -> outs[i] in directions[i]) into one CUDA graph.  Transforms with
+ * the same branches[i] run in order on one branch; different branches run
+ * concurrently (branches = NULL: every transform on its own branch), so fields
+ * of different sizes overlap.  The buffers are baked into the graph:
+ * every dfft_graph_launch repeats the same transforms on the same pointers.
+ * Plans must outlive the graph.  No counterpart in the reference (its
+ * batched Navier-Stokes example loops over execute calls). */
+typedef struct dfft_graph_s dfft_graph;
+dfft_status dfft_graph_create(dfft_graph** graph, const dfft_plan* const* plans, const void* const* ins,
+                              void* const* outs, const int32_t* directions, const int32_t* branches, int64_t count);
+dfft_status dfft_graph_launch(const dfft_graph* graph, void* stream);
+dfft_status dfft_graph_destroy(dfft_graph* graph);
+
 /* get_all_slab_topologies (pencil = 0) / get_all_pencil_topologies (pencil = 1),
  * KokkosFFT_Distributed_Topologies.hpp:421-618 / :645-811, on their own.  On
  * entry *n is the capacity (number of topologies) of the output arrays; on

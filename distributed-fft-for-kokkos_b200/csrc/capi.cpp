@@ -148,6 +148,15 @@ dfft_status dfft_execute_on_stream(const dfft_plan* plan, const void* in, void* 
   });
 }
 
+dfft_status dfft_execute_adjoint(const dfft_plan* plan, const void* in, void* out, int32_t direction, void* stream) {
+  return guarded([&] {
+    const auto& p = impl_of(plan);
+    if (direction != DFFT_FORWARD && direction != DFFT_BACKWARD)
+      dfft::fail(dfft::kErrInvalidArgument, "Invalid FFT direction specified.");
+    p.execute_adjoint(in, out, direction == DFFT_FORWARD, static_cast<cudaStream_t>(stream));
+  });
+}
+
 dfft_status dfft_execute(const dfft_plan* plan, const void* in, void* out, int32_t direction) {
   if (!plan || !plan->impl) return set_error(DFFT_ERROR_INVALID_ARGUMENT, "null plan");
   return dfft_execute_on_stream(plan, in, out, direction, plan->impl->desc().stream);

@@ -73,6 +73,10 @@ cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afa
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
 cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);
+// Multiply the interior modes (k != 0, 2k != n_real along `axis`) of a complex
+// array stored in layout L by `factor`.
+cudaError_t launch_weight(const DevLayout& L, void* data, bool dbl, int nd, const int64_t* ext, int axis, int n_real,
+                          double factor, cudaStream_t st);
 
 }  // namespace dev
 }  // namespace dfft

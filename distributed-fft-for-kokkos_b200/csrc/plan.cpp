@@ -82,6 +82,8 @@ Plan::Plan(const PlanDesc& d, bool on_device) : d_(d), on_device_(on_device) {
   try {
     build_fused(true);
     build_fused(false);
+    build_adjoint(true);
+    build_adjoint(false);
     if (d_.exec_mode == 1 || d_.exec_mode == 2) {
       prog_[0].clear();
       prog_[1].clear();
@@ -410,6 +412,82 @@ void Plan::build_fused(bool forward) {
 }
 
 // ---------------------------------------------------------------------------
+// Adjoint programs.  For C2C the adjoint of s * DFT is s * (unnormalised
+// inverse DFT), i.e. the opposite fused program with the other scale.  For
+// R2C (real x, half spectrum along the R2C axis): adjoint(R2C) = C2R * diag(1/w)
+// and adjoint(C2R) = diag(w) * R2C with w = 2 on the interior modes (doubled by
+// the Hermitian extension) and 1 on DC / Nyquist; the weights commute with the
+// C2C transforms along the other axes and are applied to a complex
+// intermediate through the layout tables.
+// ---------------------------------------------------------------------------
+void Plan::build_adjoint(bool of_forward) {
+  auto& prog = adj_[of_forward ? 0 : 1];
+  prog.clear();
+  auto order = fft_axis_order();
+  const std::size_t S = order.size();
+  const std::size_t ar = order.front();  // R2C axis
+  Layout I;
+  I.gext = d_.gout;
+  I.topo.assign(d_.gout.size(), 1);
+  I.map = identity_map(d_.gout.size());
+  I.view_right = d_.view_right;
+  I.complex = true;
+  const int li = add_layout(I), lin = add_layout(lin_), lout = add_layout(lout_);
+  const double scale = of_forward ? scale_fwd_ : scale_bwd_;
+  auto weight_op = [&](int layout, int buf, double factor) {
+    Op w;
+    w.type = Op::Weight;
+    w.src = w.dst = buf;
+    w.src_layout = layout;
+    w.w_axis = static_cast<int>(ar);
+    w.w_n = static_cast<int>(d_.gin[ar]);
+    w.scale = factor;
+    return w;
+  };
+  if (of_forward) {
+    // output layout -> input layout: inverse transforms, C2R last
+    std::reverse(order.begin(), order.end());
+    int cur_l = lout, cur_b = kBufIn;
+    if (d_.r2c && S == 1) {
+      Op c = make_stage(lout, li, layout_fast_axis(lout_), dev::kCopy, false, 1.0);
+      c.src = kBufIn;
+      c.dst = kBufScratch0;
+      prog.push_back(c);
+      prog.push_back(weight_op(li, kBufScratch0, 0.5));
+      cur_l = li;
+      cur_b = kBufScratch0;
+    }
+    for (std::size_t s = 0; s < S; ++s) {
+      const bool last = s == S - 1;
+      const int kind = (last && d_.r2c) ? dev::kC2R : dev::kC2C;
+      const int dst_l = last ? lin : li;
+      Op op = make_stage(cur_l, dst_l, order[s], kind, true, last ? scale : 1.0);
+      op.src = cur_b;
+      op.dst = last ? kBufOut : (cur_b == kBufScratch0 ? kBufScratch1 : kBufScratch0);
+      prog.push_back(op);
+      cur_l = dst_l;
+      cur_b = op.dst;
+      if (s == 0 && d_.r2c && S >= 2) prog.push_back(weight_op(li, cur_b, 0.5));
+    }
+  } else {
+    // input layout -> output layout: forward transforms, R2C first
+    int cur_l = lin, cur_b = kBufIn;
+    for (std::size_t s = 0; s < S; ++s) {
+      const bool first = s == 0, last = s == S - 1;
+      const int kind = (first && d_.r2c) ? dev::kR2C : dev::kC2C;
+      const int dst_l = last ? lout : li;
+      Op op = make_stage(cur_l, dst_l, order[s], kind, false, last ? scale : 1.0);
+      op.src = cur_b;
+      op.dst = last ? kBufOut : (cur_b == kBufScratch0 ? kBufScratch1 : kBufScratch0);
+      prog.push_back(op);
+      cur_l = dst_l;
+      cur_b = op.dst;
+      if (first && d_.r2c) prog.push_back(weight_op(cur_l, cur_b, 2.0));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Literal program (reference block sequence)
 // ---------------------------------------------------------------------------
 std::int64_t Plan::add_geo(const Layout& L, const BlockInfo& b, std::size_t pc) {
@@ -672,8 +750,8 @@ void Plan::allocate_device() {
   bufs_.assign(buf_bytes_.size(), nullptr);
   // only allocate the scratch buffers the programs use
   std::vector<bool> used(buf_bytes_.size(), false);
-  for (auto& prog : prog_)
-    for (auto& op : prog) {
+  for (auto* progs : {&prog_[0], &prog_[1], &adj_[0], &adj_[1]})
+    for (auto& op : *progs) {
       if (op.src >= kBufScratch0) used[op.src] = true;
       if (op.dst >= kBufScratch0) used[op.dst] = true;
     }
@@ -710,8 +788,9 @@ void Plan::allocate_device() {
     L.rstride = T.rstride;
     return L;
   };
-  for (auto& prog : prog_) {
-    for (auto& op : prog) {
+  for (auto* progs : {&prog_[0], &prog_[1], &adj_[0], &adj_[1]}) {
+    for (auto& op : *progs) {
+      if (op.type == Op::Weight) op.sa.dst = dev_layout(op.src_layout);
       if (op.type == Op::Stage) {
         op.sa.src = dev_layout(op.src_layout);
         op.sa.dst = dev_layout(op.dst_layout);
@@ -766,8 +845,8 @@ void Plan::autotune() {
   bool cleared = false;
   std::lock_guard<std::mutex> lock(g_tune_mutex);
   load_tune_cache_locked();
-  for (auto& prog : prog_) {
-    for (auto& op : prog) {
+  for (auto* progs : {&prog_[0], &prog_[1], &adj_[0], &adj_[1]}) {
+    for (auto& op : *progs) {
       if (op.type != Op::Stage || !op.fast) continue;
       dev::StageArgs& A = op.sa;
       std::ostringstream k;
@@ -827,7 +906,7 @@ void Plan::autotune() {
 // ---------------------------------------------------------------------------
 // Execution
 // ---------------------------------------------------------------------------
-void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream) const {
+void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, cudaStream_t stream) const {
   if (!on_device_) fail(kErrInvalidArgument, "plan was created by dfft_plan_analyze and cannot execute");
   if (!in || !out) fail(kErrInvalidArgument, "null buffer");
   if (in == out) fail(kErrInvalidArgument, "in-place execution is not supported: in and out must differ");
@@ -836,7 +915,7 @@ void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream)
     if (id == kBufOut) return out;
     return bufs_.at(id);
   };
-  for (const Op& op0 : prog_[forward ? 0 : 1]) {
+  for (const Op& op0 : prog) {
     cudaError_t e = cudaSuccess;
     switch (op0.type) {
       case Op::Stage: {
@@ -862,9 +941,25 @@ void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream)
       }
       case Op::Scale: e = dev::launch_scale(buf(op0.dst), op0.n_real, d_.dbl, op0.scale, stream); break;
       case Op::Copy: e = cudaMemcpyAsync(buf(op0.dst), buf(op0.src), op0.bytes, cudaMemcpyDeviceToDevice, stream); break;
+      case Op::Weight: {
+        const Layout& L = layouts_[op0.src_layout];
+        std::int64_t ext[4] = {1, 1, 1, 1};
+        for (std::size_t k = 0; k < L.gext.size(); ++k) ext[k] = static_cast<std::int64_t>(L.gext[k]);
+        e = dev::launch_weight(op0.sa.dst, buf(op0.dst), d_.dbl, static_cast<int>(L.gext.size()), ext, op0.w_axis,
+                               op0.w_n, op0.scale, stream);
+        break;
+      }
     }
     if (e != cudaSuccess) fail(kErrCuda, std::string("kernel launch failed: ") + cudaGetErrorString(e));
   }
+}
+
+void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream) const {
+  run_program(prog_[forward ? 0 : 1], in, out, stream);
+}
+
+void Plan::execute_adjoint(const void* in, void* out, bool of_forward, cudaStream_t stream) const {
+  run_program(adj_[of_forward ? 0 : 1], in, out, stream);
 }
 
 void Plan::export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const {

@@ -31,7 +31,7 @@ struct PlanDesc {
 enum : int { kBufIn = 0, kBufOut = 1, kBufScratch0 = 2, kBufScratch1 = 3, kBufFirstDebug = 4 };
 
 struct Op {
-  enum Type { Stage, Pack, All2All, Unpack, Scale, Copy } type;
+  enum Type { Stage, Pack, All2All, Unpack, Scale, Copy, Weight } type;
   int src = -1, dst = -1;  // buffer ids
   // Stage
   dev::StageArgs sa{};
@@ -46,6 +46,8 @@ struct Op {
   dev::XposeArgs xa{};
   int elem_bytes = 0;
   int block = -1;  // transpose block index in the block list
+  // Weight (Hermitian weights of an R2C spectrum)
+  int w_axis = 0, w_n = 0;
   // Scale / Copy
   std::int64_t n_real = 0;
   std::size_t bytes = 0;
@@ -60,6 +62,10 @@ class Plan {
   Plan& operator=(const Plan&) = delete;
 
   void execute(const void* in, void* out, bool forward, cudaStream_t stream) const;
+  // Adjoint (conjugate transpose) of the forward (of_forward) or backward
+  // transform, normalisation included: of_forward maps the output layout to the
+  // input layout, the other the input layout to the output layout.
+  void execute_adjoint(const void* in, void* out, bool of_forward, cudaStream_t stream) const;
 
   const std::string& name() const { return name_; }
   std::size_t nprocs() const { return total_size(d_.in_topo); }
@@ -97,6 +103,7 @@ class Plan {
   std::vector<std::int64_t> layout_base_;  // offset of each layout's tables
   std::int64_t* d_tables_ = nullptr;
   std::vector<Op> prog_[2];
+  std::vector<Op> adj_[2];  // adjoint of forward, adjoint of backward
   std::vector<void*> bufs_;                 // device buffers by id (in/out are null)
   std::vector<std::size_t> buf_bytes_;
   std::map<std::pair<std::size_t, bool>, void*> twiddles_;
@@ -112,6 +119,8 @@ class Plan {
   std::int64_t add_geo(const Layout& L, const BlockInfo& b, std::size_t pc);
   void build_fused(bool forward);
   void build_literal(bool forward);
+  void build_adjoint(bool of_forward);
+  void run_program(const std::vector<Op>& prog, const void* in, void* out, cudaStream_t stream) const;
   void finalize_program(std::vector<Op>& prog, int cur_layout, int cur_buf, const Layout& final_layout,
                         double scale, bool final_complex);
   void allocate_device();

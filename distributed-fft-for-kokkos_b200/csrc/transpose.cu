@@ -120,6 +120,56 @@ __global__ void scale_kernel(T* p, int64_t n, T s) {
     p[t] *= s;
 }
 
+// Hermitian weight of an R2C spectrum: every element whose index k along the
+// R2C axis is an interior mode (k != 0 and 2k != n_real) is multiplied by f.
+// Walks the global index space and addresses any layout through its tables.
+template <typename C>
+__global__ void hermitian_weight_kernel(const DevLayout L, C* data, int nd, int64_t e0, int64_t e1, int64_t e2,
+                                        int64_t e3, int axis, int n_real, double f) {
+  const int64_t total = e0 * e1 * e2 * e3;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t r = t;
+    int c[4];
+    c[3] = static_cast<int>(r % e3);
+    r /= e3;
+    c[2] = static_cast<int>(r % e2);
+    r /= e2;
+    c[1] = static_cast<int>(r % e1);
+    c[0] = static_cast<int>(r / e1);
+    int k = c[0];
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+      if (axis == q) k = c[q];
+    if (k == 0 || 2 * k == n_real) continue;
+    // logical coordinates of the nd-dimensional array sit in the last nd slots
+    int cc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cc[q] = (q < nd) ? c[q + 4 - nd] : 0;
+    C& v = data[layout_offset(L, cc, nd)];
+    v.x *= f;
+    v.y *= f;
+  }
+}
+
+static unsigned grid_for(int64_t n, int threads);
+
+cudaError_t launch_weight(const DevLayout& L, void* data, bool dbl, int nd, const int64_t* ext, int axis, int n_real,
+                          double factor, cudaStream_t st) {
+  int64_t e[4] = {1, 1, 1, 1};
+  for (int q = 0; q < nd; ++q) e[4 - nd + q] = ext[q];
+  const int a4 = axis + 4 - nd;
+  const int64_t total = e[0] * e[1] * e[2] * e[3];
+  const unsigned grid = grid_for(total, 256);
+  if (dbl)
+    hermitian_weight_kernel<double2><<<grid, 256, 0, st>>>(L, static_cast<double2*>(data), nd, e[0], e[1], e[2], e[3],
+                                                            a4, n_real, factor);
+  else
+    hermitian_weight_kernel<float2><<<grid, 256, 0, st>>>(L, static_cast<float2*>(data), nd, e[0], e[1], e[2], e[3],
+                                                           a4, n_real, factor);
+  return cudaGetLastError();
+}
+
 static unsigned grid_for(int64_t n, int threads) {
   int64_t g = (n + threads - 1) / threads;
   const int64_t cap = 148 * 32;

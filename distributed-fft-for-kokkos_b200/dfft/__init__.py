@@ -13,6 +13,7 @@ from .plan import (  # noqa: F401
     Status,
     all_topologies,
     execute,
+    execute_adjoint,
     gather_blocks,
     scatter_blocks,
 )

@@ -60,6 +60,8 @@ SIGNATURES = {
     "dfft_execute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
     "dfft_execute_on_stream": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "dfft_execute_adjoint": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     "dfft_plan_name": (ctypes.c_char_p, [ctypes.c_void_p]),
     "dfft_get_nprocs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "dfft_get_local_extents": (

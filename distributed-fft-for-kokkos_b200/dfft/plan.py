@@ -328,6 +328,15 @@ def execute(plan, in_buf, out_buf, direction, stream=None):
                                           ctypes.c_void_p(int(stream))))
 
 
+def execute_adjoint(plan, in_buf, out_buf, direction, stream=None):
+    """Adjoint (conjugate transpose, normalisation included) of the plan's
+    forward (``direction=forward``: output layout -> input layout) or backward
+    transform (input layout -> output layout)."""
+    direction = Direction(direction)
+    _check(lib.dfft_execute_adjoint(plan._h, _ptr(in_buf), _ptr(out_buf), int(direction),
+                                    ctypes.c_void_p(int(stream)) if stream else None))
+
+
 def scatter_blocks(plan, global_array, which="in"):
     """Concatenate the per-rank blocks of a global (numpy) array in rank order,
     each block in the plan's memory order."""

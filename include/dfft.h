@@ -140,6 +140,15 @@ dfft_status dfft_execute(const dfft_plan* plan, const void* in, void* out, int32
 dfft_status dfft_execute_on_stream(const dfft_plan* plan, const void* in, void* out, int32_t direction,
                                    void* stream);
 
+/* Adjoint (conjugate transpose, normalisation included) of the plan's forward
+ * (direction = DFFT_FORWARD: reads the complex output layout, writes the input
+ * layout) or backward transform (DFFT_BACKWARD: reads the input layout, writes
+ * the complex output layout).  For R2C plans the real-input adjoint weights
+ * the interior modes of the R2C axis (1/2 before C2R, 2 after R2C), so that
+ * <F x, y> = <x, F^H y> with the real inner product.  No counterpart in the
+ * reference (used for gradients through the transform). */
+dfft_status dfft_execute_adjoint(const dfft_plan* plan, const void* in, void* out, int32_t direction, void* stream);
+
 /* "SlabPlan", "PencilPlan" or "SharedPlan" (Plan::name). */
 const char* dfft_plan_name(const dfft_plan* plan);
 

@@ -9,10 +9,15 @@
 #include <vector>
 
 #include "../../include/dfft.h"
+#include "ns.hpp"
 #include "plan.hpp"
 
 struct dfft_plan_s {
   dfft::Plan* impl;
+};
+
+struct dfft_ns_s {
+  dfft::NsState* impl;
 };
 
 struct dfft_graph_s {
@@ -441,6 +446,58 @@ dfft_status dfft_graph_destroy(dfft_graph* graph) {
     if (graph->exec) cudaGraphExecDestroy(graph->exec);
     if (graph->graph) cudaGraphDestroy(graph->graph);
     delete graph;
+  });
+}
+
+dfft_status dfft_ns_create(dfft_ns** ns, const dfft_plan* plan, double nu, double dt, double lx) {
+  return guarded([&] {
+    if (!ns) dfft::fail(dfft::kErrInvalidArgument, "null output pointer");
+    *ns = nullptr;
+    const auto& p = impl_of(plan);
+    if (!p.on_device()) dfft::fail(dfft::kErrInvalidArgument, "plan was created by dfft_plan_analyze");
+    auto* impl = dfft::ns_create(&p, nu, dt, lx);
+    *ns = new dfft_ns_s{impl};
+  });
+}
+
+static dfft::NsState* ns_of(dfft_ns* ns) {
+  if (!ns || !ns->impl) dfft::fail(dfft::kErrInvalidArgument, "null Navier-Stokes state");
+  return ns->impl;
+}
+
+dfft_status dfft_ns_init_taylor_green(dfft_ns* ns, void* uk, double v0, void* stream) {
+  return guarded([&] {
+    if (!uk) dfft::fail(dfft::kErrInvalidArgument, "null buffer");
+    dfft::ns_taylor_green(ns_of(ns), uk, v0, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_ns_rhs(dfft_ns* ns, void* uk, void* dukdt, void* stream) {
+  return guarded([&] {
+    if (!uk || !dukdt) dfft::fail(dfft::kErrInvalidArgument, "null buffer");
+    dfft::ns_rhs(ns_of(ns), uk, dukdt, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_ns_step(dfft_ns* ns, void* uk, void* stream) {
+  return guarded([&] {
+    if (!uk) dfft::fail(dfft::kErrInvalidArgument, "null buffer");
+    dfft::ns_step(ns_of(ns), uk, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_ns_energy(dfft_ns* ns, const void* uk, double* energy, void* stream) {
+  return guarded([&] {
+    if (!uk || !energy) dfft::fail(dfft::kErrInvalidArgument, "null argument");
+    *energy = dfft::ns_energy(ns_of(ns), uk, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_ns_destroy(dfft_ns* ns) {
+  return guarded([&] {
+    if (!ns) return;
+    dfft::ns_destroy(ns->impl);
+    delete ns;
   });
 }
 

@@ -962,6 +962,29 @@ void Plan::execute_adjoint(const void* in, void* out, bool of_forward, cudaStrea
   run_program(adj_[of_forward ? 0 : 1], in, out, stream);
 }
 
+dev::DevLayout Plan::device_layout(bool output) const {
+  if (!on_device_) fail(kErrInvalidArgument, "plan has no device tables");
+  Layout L = output ? lout_ : lin_;
+  for (std::size_t i = 0; i < layouts_.size(); ++i) {
+    if (layouts_[i] == L) {
+      dev::DevLayout D;
+      std::memset(&D, 0, sizeof(D));
+      const LayoutTables& T = tables_[i];
+      D.t = d_tables_ + layout_base_[i];
+      D.mode = T.mode;
+      for (int k = 0; k < 4; ++k) {
+        D.off[k] = T.off[k];
+        D.rk[k] = T.rk[k];
+        D.loc[k] = T.loc[k];
+      }
+      D.rbase = T.rbase;
+      D.rstride = T.rstride;
+      return D;
+    }
+  }
+  fail(kErrInternal, "layout not registered");
+}
+
 void Plan::export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const {
   if (!on_device_) fail(kErrInvalidArgument, "plan has no device buffers");
   if (which < 0 || which > 3) fail(kErrInvalidArgument, "which must be 0 (send), 1 (recv), 2 (pack input) or 3 (unpack output)");

@@ -80,6 +80,8 @@ class Plan {
   std::size_t launches(bool forward) const { return prog_[forward ? 0 : 1].size(); }
   std::size_t workspace_bytes() const { return workspace_bytes_; }
   bool on_device() const { return on_device_; }
+  // Device tables of the caller-facing input / output layouts.
+  dev::DevLayout device_layout(bool output) const;
   // Copy a buffer recorded by a capturing literal execution of transpose
   // block `block` to host: which = 0 send, 1 recv, 2 pack input, 3 unpack output.
   void export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const;

@@ -97,6 +97,15 @@ SIGNATURES = {
                        ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.c_int64]),
     "dfft_graph_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "dfft_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dfft_ns_create": (
+        ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                       ctypes.c_double]),
+    "dfft_ns_init_taylor_green": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]),
+    "dfft_ns_rhs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_ns_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_ns_energy": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "dfft_ns_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dfft_last_error_string": (ctypes.c_char_p, []),
     "dfft_version": (ctypes.c_char_p, []),
 }

@@ -1,0 +1,49 @@
+"""Pseudo-spectral Navier-Stokes step of the reference's batched example
+(``examples/navier-stokes-MPI-batched/main.cpp``) on a distributed R2C plan.
+
+The plan transforms the velocity field, a LayoutRight 4D view (3, nx, ny, nz),
+over axes (1, 2, 3); ``uk`` is the plan's output (spectral) buffer.  The
+reference builds the same plan with in_topology (1, px, py, 1) and
+out_topology (1, 1, px, py) (main.cpp:96-102).
+"""
+import ctypes
+
+from ._lib import lib
+from .plan import _check, _ptr
+
+
+class NavierStokes:
+    """``NavierStokes(plan, nu, dt, lx)``: nu = 1 / Re, dt the time step, the
+    domain [0, lx pi)^3.  Methods mirror the example's NavierStokes / RK4th
+    members: ``init_taylor_green`` (Variables constructor, main.cpp:322-363),
+    ``rhs`` (main.cpp:536-586), ``step`` (solve, main.cpp:518-528) and
+    ``energy`` (diag_energy, main.cpp:746-766)."""
+
+    def __init__(self, plan, nu=0.01, dt=0.01, lx=2.0):
+        self._plan = plan  # the plan must outlive the state
+        self._h = ctypes.c_void_p()
+        _check(lib.dfft_ns_create(ctypes.byref(self._h), plan._h, float(nu), float(dt), float(lx)))
+
+    @staticmethod
+    def _stream(stream):
+        return ctypes.c_void_p(int(stream)) if stream else None
+
+    def init_taylor_green(self, uk, v0=1.0, stream=None):
+        _check(lib.dfft_ns_init_taylor_green(self._h, _ptr(uk), float(v0), self._stream(stream)))
+
+    def rhs(self, uk, dukdt, stream=None):
+        _check(lib.dfft_ns_rhs(self._h, _ptr(uk), _ptr(dukdt), self._stream(stream)))
+
+    def step(self, uk, stream=None):
+        _check(lib.dfft_ns_step(self._h, _ptr(uk), self._stream(stream)))
+
+    def energy(self, uk, stream=None):
+        e = ctypes.c_double(0.0)
+        _check(lib.dfft_ns_energy(self._h, _ptr(uk), ctypes.byref(e), self._stream(stream)))
+        return e.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dfft_ns_destroy(h)
+            self._h = None

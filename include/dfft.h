@@ -196,6 +196,27 @@ dfft_status dfft_graph_create(dfft_graph** graph, const dfft_plan* const* plans,
 dfft_status dfft_graph_launch(const dfft_graph* graph, void* stream);
 dfft_status dfft_graph_destroy(dfft_graph* graph);
 
+/* ---- Pseudo-spectral Navier-Stokes step of the reference's batched example
+ * (examples/navier-stokes-MPI-batched/main.cpp:518-669, RK4 of
+ * examples/utils/math_utils.hpp:90-141) on a plan's buffers.  The plan must be
+ * an R2C plan over LayoutRight 4D views (3, nx, ny, nz) with FFT axes {1,2,3};
+ * uk is its output (spectral) buffer.  nu = 1/Re, dt the time step, the
+ * domain is [0, lx*pi)^3 (lx = 2 for [0, 2 pi)). */
+typedef struct dfft_ns_s dfft_ns;
+dfft_status dfft_ns_create(dfft_ns** ns, const dfft_plan* plan, double nu, double dt, double lx);
+/* Taylor-Green vortex (main.cpp:322-363): u = (v0 sin x cos y cos z,
+ * -v0 cos x sin y cos z, 0) on x = lx pi i / nx, uk = its forward transform,
+ * dealiased and projected onto the divergence-free space */
+dfft_status dfft_ns_init_taylor_green(dfft_ns* ns, void* uk, double v0, void* stream);
+/* dukdt = right-hand side at uk (uk is dealiased in place, as in the reference) */
+dfft_status dfft_ns_rhs(dfft_ns* ns, void* uk, void* dukdt, void* stream);
+/* one RK4 time step of uk in place (4 right-hand sides: 20 transforms) */
+dfft_status dfft_ns_step(dfft_ns* ns, void* uk, void* stream);
+/* total kinetic energy of main.cpp:746-766, (lx pi)^3 / N^2 * sum 0.5 factor |uk|^2
+ * (factor 1 on kz = 0, else 2), FP64 reduction; synchronises the stream */
+dfft_status dfft_ns_energy(dfft_ns* ns, const void* uk, double* energy, void* stream);
+dfft_status dfft_ns_destroy(dfft_ns* ns);
+
 /* get_all_slab_topologies (pencil = 0) / get_all_pencil_topologies (pencil = 1),
  * KokkosFFT_Distributed_Topologies.hpp:421-618 / :645-811, on their own.  On
  * entry *n is the capacity (number of topologies) of the output arrays; on

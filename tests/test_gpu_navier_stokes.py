@@ -1,0 +1,125 @@
+"""Navier-Stokes step of the reference's batched example on the GPU plan,
+against the numpy oracle (ns_oracle) on the same inputs.
+
+The plan is the example's: R2C over LayoutRight 4D views (3, nx, ny, nz),
+axes (1, 2, 3), in_topology (1, px, py, 1), out_topology (1, 1, px, py)
+(examples/navier-stokes-MPI-batched/main.cpp:96-102, 476-479).  Checked:
+the Taylor-Green initial spectrum, one right-hand side (and the in-place
+dealiasing of uk), two RK4 steps, the kinetic energy, and the energy decay
+of the vortex against exp(-6 nu t).  Tolerances: relative L2 <= 1e-12 for
+float64, <= 1e-5 for float32."""
+import numpy as np
+import pytest
+
+import dfft
+import ns_oracle as N
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ((16, 16, 16), (1, 2, 1, 1), (1, 1, 2, 1)),   # slab, px = 2 (the example's default split)
+    ((16, 16, 16), (1, 2, 2, 1), (1, 1, 2, 2)),   # pencil 2 x 2
+    ((24, 20, 18), (1, 3, 2, 1), (1, 1, 3, 2)),   # ragged pencil 3 x 2
+    ((16, 14, 20), (1, 1, 1, 1), (1, 1, 1, 1)),   # one rank
+]
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b)))
+
+
+def _setup(shape, tin, tout, precision):
+    import torch
+    nx, ny, nz = shape
+    plan = dfft.Plan((3, nx, ny, nz), (3, nx, ny, nz // 2 + 1), (1, 2, 3), tin, tout, real_input=True,
+                     precision=precision)
+    cdt = torch.complex128 if precision == "float64" else torch.complex64
+    return plan, cdt
+
+
+def _to_dev(plan, a, cdt):
+    import torch
+    np_c = np.complex128 if cdt == torch.complex128 else np.complex64
+    return torch.from_numpy(np.ascontiguousarray(dfft.scatter_blocks(plan, a.astype(np_c), "out"))).cuda()
+
+
+def _to_host(plan, t):
+    import torch
+    torch.cuda.synchronize()
+    return dfft.gather_blocks(plan, t.cpu().numpy(), "out").astype(np.complex128)
+
+
+def _random_spectrum(shape, seed, lx):
+    rng = np.random.default_rng(seed)
+    u = rng.standard_normal((3,) + shape)
+    k, _, inv_ksq = N.wavenumbers(*shape, lx)
+    return N.projection(np.fft.rfftn(u, axes=(1, 2, 3)), k, inv_ksq)
+
+
+@pytest.mark.parametrize("shape,tin,tout", CASES)
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_ns_matches_oracle(shape, tin, tout, precision):
+    import torch
+    lx, nu, dt = 2.0, 0.01, 0.01
+    tol = 1e-12 if precision == "float64" else 1e-5
+    plan, cdt = _setup(shape, tin, tout, precision)
+    ns = dfft.NavierStokes(plan, nu=nu, dt=dt, lx=lx)
+    nout = plan.buffer_elements("out")
+
+    # Taylor-Green initial condition and its energy
+    uk = torch.empty(nout, dtype=cdt, device="cuda")
+    ns.init_taylor_green(uk, v0=1.0)
+    _, ref_tg = N.taylor_green(*shape, lx)
+    assert _rel(_to_host(plan, uk), ref_tg) <= tol
+    e = ns.energy(uk)
+    assert abs(e / N.energy(ref_tg, lx, shape) - 1.0) <= tol
+
+    # one right-hand side of a random divergence-free field (not dealiased:
+    # rhs dealiases uk in place, as the reference does)
+    y = _random_spectrum(shape, 7, lx)
+    uk = _to_dev(plan, y, cdt)
+    dukdt = torch.empty_like(uk)
+    ns.rhs(uk, dukdt)
+    ref_ukd, ref_r = N.rhs(y, nu, lx, shape)
+    assert _rel(_to_host(plan, uk), ref_ukd) <= tol
+    assert _rel(_to_host(plan, dukdt), ref_r) <= tol
+
+    # two RK4 steps
+    uk = _to_dev(plan, y, cdt)
+    ref = y
+    for _ in range(2):
+        ns.step(uk)
+        ref = N.rk4_step(ref, nu, dt, lx, shape)
+    assert _rel(_to_host(plan, uk), ref) <= tol * 10
+    assert abs(ns.energy(uk) / N.energy(ref, lx, shape) - 1.0) <= tol * 10
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_taylor_green_decay(precision):
+    """E(t) / E(0) of the vortex follows exp(-2 nu |k|^2 t), |k|^2 = 3, over
+    short times; E(0) = (lx pi)^3 / 8."""
+    import torch
+    n, lx, nu, dt, steps = 32, 2.0, 0.01, 0.01, 10
+    plan, cdt = _setup((n, n, n), (1, 2, 2, 1), (1, 1, 2, 2), precision)
+    ns = dfft.NavierStokes(plan, nu=nu, dt=dt, lx=lx)
+    uk = torch.empty(plan.buffer_elements("out"), dtype=cdt, device="cuda")
+    ns.init_taylor_green(uk)
+    e0 = ns.energy(uk)
+    assert abs(e0 / np.pi ** 3 - 1.0) < (1e-13 if precision == "float64" else 1e-6)
+    prev = e0
+    for _ in range(steps):
+        ns.step(uk)
+        e = ns.energy(uk)
+        assert e < prev
+        prev = e
+    ratio = prev / e0
+    assert abs(ratio / np.exp(-6.0 * nu * steps * dt) - 1.0) < (1e-5 if precision == "float64" else 1e-4)
+
+
+def test_ns_rejects_wrong_plan():
+    plan = dfft.Plan((16, 16, 16), (16, 16, 9), (0, 1, 2), (2, 1, 1), (1, 2, 1), real_input=True)
+    with pytest.raises(dfft.DistributedFFTError):
+        dfft.NavierStokes(plan)
+    plan = dfft.Plan((3, 16, 16, 16), (3, 16, 16, 16), (1, 2, 3), (1, 2, 1, 1), (1, 1, 2, 1))
+    with pytest.raises(dfft.DistributedFFTError):
+        dfft.NavierStokes(plan)

@@ -1,4 +1,4 @@
-// Register-resident FFT stage for power-of-two lines (sm_100a).
+// Register-resident FFT stage for lines of 2^k or 3 * 2^k points (sm_100a).
 //
 // Used when both the source and the destination address every tile row as a
 // contiguous run: either every line is contiguous (unit stride along the FFT
@@ -7,7 +7,9 @@
 // offsets come from the separable layout tables, so the stage still performs
 // the reference's pack / all-to-all / unpack / local transpose by addressing.
 //
-// Each line of length N is transformed by N/8 threads holding 8 values each.
+// Each line of length N is transformed by N/V threads holding V values each
+// (V = 8 for powers of two, V = 24 for 3 * 2^k; every radix of the plan
+// divides V, so each pass is V/R butterflies per thread).
 // The first radix pass reads its inputs straight from global memory and the
 // last pass writes its outputs straight to global memory (consecutive threads
 // touch consecutive addresses for either row orientation); the passes in
@@ -57,9 +59,23 @@ __device__ __forceinline__ void r8(cplx<T>* v) {
   v[7] = csub(e3, t3);
 }
 
+template <typename T, bool INV>
+__device__ __forceinline__ void r3(cplx<T>* v) {
+  using C = cplx<T>;
+  const T c3 = T(0.86602540378443864676372317075293618347);  // sqrt(3)/2
+  const C t = cadd(v[1], v[2]);
+  const C d = rot<INV>(cscale(csub(v[1], v[2]), c3));
+  const C m = csub(v[0], cscale(t, T(0.5)));
+  v[0] = cadd(v[0], t);
+  v[1] = cadd(m, d);
+  v[2] = csub(m, d);
+}
+
 template <typename T, bool INV, int R>
 __device__ __forceinline__ void dftR(cplx<T>* v) {
-  if constexpr (R == 2) {
+  if constexpr (R == 3) {
+    r3<T, INV>(v);
+  } else if constexpr (R == 2) {
     const cplx<T> t = v[0];
     v[0] = cadd(t, v[1]);
     v[1] = csub(t, v[1]);
@@ -70,8 +86,8 @@ __device__ __forceinline__ void dftR(cplx<T>* v) {
   }
 }
 
-// radix of pass P of an N-point plan: the first and the last pass are radix 8
-// whenever N allows it; all radices divide 8.
+// radix of pass P of an N-point plan: the first pass is radix 8 whenever N
+// allows it; the radix-3 pass of 3 * 2^k plans is the last one.
 template <int N, int P>
 struct Radix;
 #define DFFT_PLAN(N_, ...)                                       \
@@ -90,7 +106,19 @@ DFFT_PLAN(512, 8, 8, 8)
 DFFT_PLAN(1024, 8, 4, 4, 8)
 DFFT_PLAN(2048, 8, 4, 8, 8)
 DFFT_PLAN(4096, 8, 8, 8, 8)
+DFFT_PLAN(24, 8, 3)
+DFFT_PLAN(48, 8, 2, 3)
+DFFT_PLAN(96, 8, 4, 3)
+DFFT_PLAN(192, 8, 8, 3)
+DFFT_PLAN(384, 8, 4, 4, 3)
+DFFT_PLAN(768, 8, 8, 4, 3)
 #undef DFFT_PLAN
+
+// values per thread
+template <int N>
+struct Vals {
+  static constexpr int value = (N % 3 == 0) ? 24 : 8;
+};
 
 template <int N, int P>
 struct NsOf {
@@ -144,7 +172,7 @@ __device__ __forceinline__ void compute_pass(cplx<T>* v, int t, const cplx<T>* t
   using C = cplx<T>;
   constexpr int R = Radix<N, P>::value;
   constexpr int Ns = NsOf<N, P>::value;
-  constexpr int Q = 8 / R;
+  constexpr int Q = Vals<N>::value / R;
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     if (Ns > 1) {
@@ -182,8 +210,9 @@ __device__ __forceinline__ void compute_pass(cplx<T>* v, int t, const cplx<T>* t
 
 template <typename T, bool INV, int N, int P, int TT, int S>
 __device__ __forceinline__ void exchange(cplx<T>* v, int t, cplx<T>* line) {
-  constexpr int R = Radix<N, P>::value, Q = 8 / R;
-  constexpr int R2 = Radix<N, P + 1>::value, Q2 = 8 / R2;
+  constexpr int V = Vals<N>::value;
+  constexpr int R = Radix<N, P>::value, Q = V / R;
+  constexpr int R2 = Radix<N, P + 1>::value, Q2 = V / R2;
 #pragma unroll
   for (int q = 0; q < Q; ++q)
 #pragma unroll
@@ -216,11 +245,12 @@ __device__ __forceinline__ int64_t pick(const int64_t* a, int i) {
 
 }  // namespace
 
-// B lines per CTA, N/8 threads per line.
+// B lines per CTA, N/V threads per line.
 template <typename T, bool INV, int N, int B, bool AFAST>
-__global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) {
+__global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const StageArgs A) {
   using C = cplx<T>;
-  constexpr int TT = N / 8;                  // threads per line
+  constexpr int V = Vals<N>::value;
+  constexpr int TT = N / V;                  // threads per line
   constexpr int NPASS = Radix<N, 0>::npass;
   using SH = SmemShape<T, N, B, AFAST>;
   constexpr int LP = SH::LP;
@@ -267,8 +297,8 @@ __global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) 
     dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
   }
 
-  C v[8];
-  constexpr int R0 = Radix<N, 0>::value, Q0 = 8 / R0;
+  C v[V];
+  constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
   const C* in = reinterpret_cast<const C*>(A.in);
   if (active) {
     if (AFAST) {
@@ -286,13 +316,13 @@ __global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) 
     }
   } else {
 #pragma unroll
-    for (int e = 0; e < 8; ++e) v[e] = mk<T>(T(0), T(0));
+    for (int e = 0; e < V; ++e) v[e] = mk<T>(T(0), T(0));
   }
   __syncthreads();  // twiddles staged
 
   run_fft<T, INV, N, 0, TT, SH::S>(v, t, tw, tile + line * LP);
 
-  constexpr int RL = Radix<N, NPASS - 1>::value, QL = 8 / RL;
+  constexpr int RL = Radix<N, NPASS - 1>::value, QL = V / RL;
   const T s = T(A.scale);
   C* out = reinterpret_cast<C*>(A.out);
   if (active) {
@@ -315,12 +345,13 @@ __global__ void __launch_bounds__(N / 8 * B) fft_fast_kernel(const StageArgs A) 
 
 // Default lines per CTA: at least 128-byte rows for b-fast tiles (16
 // complex64 or 8 complex128), at least 256 threads, at most 1024 threads
-// (N/8 per line).  The launcher also has variants with 1/2 and 1/4 of it.
+// (N/V per line).  The launcher also has variants with 1/2 and 1/4 of it.
 template <typename T>
 constexpr int fast_lines(int n) {
+  const int tt = n % 3 == 0 ? n / 24 : n / 8;
   const int rows = sizeof(T) == 4 ? 16 : 8;
-  const int want = rows > 2048 / n ? rows : 2048 / n;
-  const int cap = 8192 / n;
+  const int want = rows > 256 / tt ? rows : 256 / tt;
+  const int cap = 1024 / tt;
   return want < cap ? want : cap;
 }
 
@@ -336,7 +367,7 @@ static cudaError_t launch_fast_b(const StageArgs& A, unsigned tiles, cudaStream_
     if (e != cudaSuccess) return e;
     attr_bytes = smem;
   }
-  k<<<tiles, N / 8 * B, smem, st>>>(A);
+  k<<<tiles, N / Vals<N>::value * B, smem, st>>>(A);
   return cudaGetLastError();
 }
 
@@ -371,7 +402,8 @@ int fast_stage_line_options(bool dbl, int n, int* opts) {
 }
 
 bool fast_stage_supported(int n) {
-  return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096;
+  return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096 ||
+         n == 24 || n == 48 || n == 96 || n == 192 || n == 384 || n == 768;
 }
 
 cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, unsigned tiles,
@@ -390,6 +422,12 @@ cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afa
     DFFT_CASE(1024)
     DFFT_CASE(2048)
     DFFT_CASE(4096)
+    DFFT_CASE(24)
+    DFFT_CASE(48)
+    DFFT_CASE(96)
+    DFFT_CASE(192)
+    DFFT_CASE(384)
+    DFFT_CASE(768)
     default: return cudaErrorInvalidValue;
   }
 #undef DFFT_CASE

@@ -218,7 +218,7 @@ def test_input_not_modified_and_errors():
 
 
 @pytest.mark.parametrize("precision", ["float64", "float32"])
-@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 1024, 2048, 4096])
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 24, 48, 96, 192, 384, 768])
 def test_register_kernel_line_lengths(n, precision):
     # lines along the unit-stride axis (a-fast rows) and across it (b-fast rows),
     # on a slab exchange so the rows also cross virtual-rank blocks

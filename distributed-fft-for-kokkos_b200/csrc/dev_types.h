@@ -68,6 +68,10 @@ bool fast_stage_supported(int n);
 int fast_stage_lines(bool dbl, int n);
 // Lines-per-CTA variants the launcher accepts (A.B must be one of them).
 int fast_stage_line_options(bool dbl, int n, int* opts);
+// R2C first stage (c2r = false) or C2R last stage (c2r = true) of the
+// register-resident kernel; lines contiguous on both sides; A.B complex lines
+// (2 A.B real lines) per tile
+cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, unsigned tiles, cudaStream_t st);
 cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, unsigned tiles,
                             cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack

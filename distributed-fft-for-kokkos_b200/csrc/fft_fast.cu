@@ -343,6 +343,140 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
   }
 }
 
+// Real-to-complex first stage / complex-to-real last stage on lines that are
+// contiguous on both sides.  Each CTA line carries two real lines of the tile
+// (rows 2l and 2l+1 along the tile axis) as one complex line z = x0 + i x1.
+//   R2C: the N-point FFT of z goes to shared memory, and the two half spectra
+//        X0[k] = (Z[k] + conj Z[N-k]) / 2, X1[k] = (Z[k] - conj Z[N-k]) / 2i,
+//        k = 0..N/2, are written with the scale folded in.
+//   C2R: Z[k] = X0[k] + i X1[k] and Z[N-k] = conj X0[k] + i conj X1[k] are
+//        assembled in shared memory (imaginary parts of DC and Nyquist
+//        dropped), inverse FFT, x0 = Re z and x1 = Im z are written.
+template <typename T, bool C2R, int N, int B>
+__global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const StageArgs A) {
+  using C = cplx<T>;
+  constexpr int V = Vals<N>::value;
+  constexpr int TT = N / V;
+  constexpr int NPASS = Radix<N, 0>::npass;
+  constexpr int H = N / 2;
+  using SH = SmemShape<T, N, B, true>;
+  constexpr int LP = SH::LP;
+  constexpr int S = SH::S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* tile = tw + N;
+  const DevLayout ls = A.src, ld = A.dst;
+
+  int tb = blockIdx.x % A.tiles_b;
+  int rest = blockIdx.x / A.tiles_b;
+  int co0 = 0, co1 = 0;
+  if (A.o0 >= 0) {
+    co0 = rest % A.Eo0;
+    rest /= A.Eo0;
+  }
+  if (A.o1 >= 0) co1 = rest;
+  const int b0 = tb * 2 * B;               // first real line of the tile
+  const int nbr = min(2 * B, A.Eb - b0);   // real lines in the tile
+  const int t = threadIdx.x % TT;
+  const int line = threadIdx.x / TT;
+  const int r0 = 2 * line, r1 = 2 * line + 1;
+  const bool act0 = r0 < nbr, act1 = r1 < nbr;
+  C* ln = tile + line * LP;
+
+  {
+    const C* gtw = reinterpret_cast<const C*>(A.tw);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  }
+  int64_t so = 0, dof = 0;
+  if (A.o0 >= 0) {
+    so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
+    dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+  }
+  if (A.o1 >= 0) {
+    so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
+    dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+  }
+  const int64_t sa0 = __ldg(ls.t + pick(ls.off, A.a)), da0 = __ldg(ld.t + pick(ld.off, A.a));
+  const int64_t sb0 = act0 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r0) : 0;
+  const int64_t sb1 = act1 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r1) : 0;
+  const int64_t db0 = act0 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r0) : 0;
+  const int64_t db1 = act1 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r1) : 0;
+  const T s = T(A.scale);
+
+  C v[V];
+  constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
+  if constexpr (!C2R) {
+    const T* in = reinterpret_cast<const T*>(A.in);
+    const T* row0 = in + so + sb0 + sa0;
+    const T* row1 = in + so + sb1 + sa0;
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int p = in_pos<N, 0, TT>(t, q, r);
+        v[q * R0 + r] = mk<T>(act0 ? row0[p] : T(0), act1 ? row1[p] : T(0));
+      }
+    __syncthreads();  // twiddles staged
+  } else {
+    const C* in = reinterpret_cast<const C*>(A.in);
+    const C* row0 = in + so + sb0 + sa0;
+    const C* row1 = in + so + sb1 + sa0;
+    for (int k = t; k <= H; k += TT) {
+      const C x0 = act0 ? row0[k] : mk<T>(T(0), T(0));
+      const C x1 = act1 ? row1[k] : mk<T>(T(0), T(0));
+      if (k == 0 || k == H) {
+        ln[padpos<S>(k)] = mk<T>(x0.x, x1.x);
+      } else {
+        ln[padpos<S>(k)] = mk<T>(x0.x - x1.y, x0.y + x1.x);
+        ln[padpos<S>(N - k)] = mk<T>(x0.x + x1.y, x1.x - x0.y);
+      }
+    }
+    __syncthreads();  // spectrum and twiddles staged
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[q * R0 + r] = ln[padpos<S>(in_pos<N, 0, TT>(t, q, r))];
+    __syncthreads();  // every line read before the first exchange overwrites it
+  }
+
+  run_fft<T, C2R, N, 0, TT, S>(v, t, tw, ln);
+
+  constexpr int RL = Radix<N, NPASS - 1>::value, QL = V / RL;
+  if constexpr (!C2R) {
+    // the last exchange ended with a barrier: the line buffer is free
+#pragma unroll
+    for (int q = 0; q < QL; ++q)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) ln[padpos<S>(out_pos<N, NPASS - 1, TT>(t, q, r))] = v[q * RL + r];
+    __syncthreads();
+    C* out = reinterpret_cast<C*>(A.out);
+    C* row0 = out + dof + db0 + da0;
+    C* row1 = out + dof + db1 + da0;
+    const T hs = T(0.5) * s;
+    for (int k = t; k <= H; k += TT) {
+      const C z = ln[padpos<S>(k)];
+      const C zc = cconj(ln[padpos<S>(k == 0 ? 0 : N - k)]);
+      if (act0) row0[k] = cscale(cadd(z, zc), hs);
+      if (act1) {
+        const C d = csub(z, zc);
+        row1[k] = mk<T>(d.y * hs, -d.x * hs);
+      }
+    }
+  } else {
+    T* out = reinterpret_cast<T*>(A.out);
+    T* row0 = out + dof + db0 + da0;
+    T* row1 = out + dof + db1 + da0;
+#pragma unroll
+    for (int q = 0; q < QL; ++q)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int p = out_pos<N, NPASS - 1, TT>(t, q, r);
+        if (act0) row0[p] = v[q * RL + r].x * s;
+        if (act1) row1[p] = v[q * RL + r].y * s;
+      }
+  }
+}
+
 // Default lines per CTA: at least 128-byte rows for b-fast tiles (16
 // complex64 or 8 complex128), at least 256 threads, at most 1024 threads
 // (N/V per line).  The launcher also has variants with 1/2 and 1/4 of it.
@@ -390,6 +524,32 @@ static cudaError_t launch_fast_t(const StageArgs& A, bool inverse, bool afast, u
   return afast ? launch_fast_n<T, N, false, true>(A, tiles, st) : launch_fast_n<T, N, false, false>(A, tiles, st);
 }
 
+template <typename T, int N, bool C2R, int B>
+static cudaError_t launch_real_b(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+  constexpr int LP = SmemShape<T, N, B, true>::LP;
+  const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
+  auto k = fft_real_kernel<T, C2R, N, B>;
+  static size_t attr_bytes = 48 * 1024;
+  if (smem > attr_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    attr_bytes = smem;
+  }
+  k<<<tiles, N / Vals<N>::value * B, smem, st>>>(A);
+  return cudaGetLastError();
+}
+
+template <typename T, int N, bool C2R>
+static cudaError_t launch_real_n(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+  constexpr int B0 = fast_lines<T>(N);
+  constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
+  constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
+  if (A.B == B0) return launch_real_b<T, N, C2R, B0>(A, tiles, st);
+  if (A.B == B1) return launch_real_b<T, N, C2R, B1>(A, tiles, st);
+  if (A.B == B2) return launch_real_b<T, N, C2R, B2>(A, tiles, st);
+  return cudaErrorInvalidValue;
+}
+
 int fast_stage_lines(bool dbl, int n) { return dbl ? fast_lines<double>(n) : fast_lines<float>(n); }
 
 int fast_stage_line_options(bool dbl, int n, int* opts) {
@@ -412,6 +572,32 @@ cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afa
   case N_:                                                                            \
     return dbl ? launch_fast_t<double, N_>(A, inverse, afast, tiles, st)              \
                : launch_fast_t<float, N_>(A, inverse, afast, tiles, st);
+  switch (A.n) {
+    DFFT_CASE(16)
+    DFFT_CASE(32)
+    DFFT_CASE(64)
+    DFFT_CASE(128)
+    DFFT_CASE(256)
+    DFFT_CASE(512)
+    DFFT_CASE(1024)
+    DFFT_CASE(2048)
+    DFFT_CASE(4096)
+    DFFT_CASE(24)
+    DFFT_CASE(48)
+    DFFT_CASE(96)
+    DFFT_CASE(192)
+    DFFT_CASE(384)
+    DFFT_CASE(768)
+    default: return cudaErrorInvalidValue;
+  }
+#undef DFFT_CASE
+}
+
+cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, unsigned tiles, cudaStream_t st) {
+#define DFFT_CASE(N_)                                                                          \
+  case N_:                                                                                     \
+    if (dbl) return c2r ? launch_real_n<double, N_, true>(A, tiles, st) : launch_real_n<double, N_, false>(A, tiles, st); \
+    return c2r ? launch_real_n<float, N_, true>(A, tiles, st) : launch_real_n<float, N_, false>(A, tiles, st);
   switch (A.n) {
     DFFT_CASE(16)
     DFFT_CASE(32)

@@ -299,7 +299,14 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   std::size_t b;
   if (fd != a) b = fd;
   else if (fs != a) b = fs;
-  else b = (a == 0) ? 1 : 0;
+  else {
+    // lines contiguous on both sides: tile along the longest other axis so
+    // that short axes (e.g. the 3 components of a batched 4D view) do not
+    // leave most lines of a tile empty
+    b = (a == 0) ? 1 : 0;
+    for (std::size_t k = 0; k < D; ++k)
+      if (k != a && Dl.gext[k] > Dl.gext[b]) b = k;
+  }
   A.b = static_cast<int>(b);
   int others[2] = {-1, -1}, no = 0;
   for (std::size_t k = 0; k < D; ++k)
@@ -373,7 +380,36 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
       op.tiles = static_cast<unsigned>(ft);
     }
   }
+  // Register-resident R2C (first) / C2R (last) stage: lines contiguous on
+  // both sides, every line a complete run of n reals / n/2+1 complex values.
+  if ((kind == dev::kR2C || kind == dev::kC2R) && dev::fast_stage_supported(static_cast<int>(n)) && A.load_afast &&
+      A.store_afast && tables_[src_l].mode == 0 && tables_[dst_l].mode == 0) {
+    const std::size_t nr = n, nc = n / 2 + 1;
+    const std::size_t ns = kind == dev::kR2C ? nr : nc, nd = kind == dev::kR2C ? nc : nr;
+    auto run_ok = [&](const LayoutTables& T, std::size_t len) {
+      const std::int64_t* off = T.data.data() + T.off[a];
+      for (std::size_t c = 1; c < len; ++c)
+        if (off[c] != off[0] + static_cast<std::int64_t>(c)) return false;
+      return true;
+    };
+    if (S.gext[a] == ns && Dl.gext[a] == nd && run_ok(tables_[src_l], ns) && run_ok(tables_[dst_l], nd)) {
+      const std::size_t Bf = static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)));
+      op.fast = true;
+      A.B = static_cast<int>(Bf);
+      A.tiles_b = static_cast<int>((Dl.gext[b] + 2 * Bf - 1) / (2 * Bf));
+      const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
+      if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
+      op.tiles = static_cast<unsigned>(ft);
+    }
+  }
   return op;
+}
+
+// Launch of a register-resident stage (C2C, R2C or C2R).
+static cudaError_t launch_fast_op(const dev::StageArgs& A, bool dbl, int kind, bool inverse, unsigned tiles,
+                                  cudaStream_t st) {
+  if (kind == dev::kR2C || kind == dev::kC2R) return dev::launch_fft_fast_real(A, dbl, kind == dev::kC2R, tiles, st);
+  return dev::launch_fft_fast(A, dbl, inverse, A.load_afast != 0, tiles, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -850,12 +886,14 @@ void Plan::autotune() {
       if (op.type != Op::Stage || !op.fast) continue;
       dev::StageArgs& A = op.sa;
       std::ostringstream k;
+      const bool pairs = op.kind == dev::kR2C || op.kind == dev::kC2R;
       k << "fast:n" << A.n << (d_.dbl ? "f64" : "f32") << (op.inverse ? "i" : "f") << (A.load_afast ? "a" : "b")
-        << ":" << A.Eb << "x" << A.Eo0 << "x" << A.Eo1;
+        << (op.kind == dev::kR2C ? "r2c" : op.kind == dev::kC2R ? "c2r" : "") << ":" << A.Eb << "x" << A.Eo0 << "x"
+        << A.Eo1;
       const std::string key = k.str();
       auto apply = [&](int B) {
         A.B = B;
-        A.tiles_b = (A.Eb + B - 1) / B;
+        A.tiles_b = pairs ? (A.Eb + 2 * B - 1) / (2 * B) : (A.Eb + B - 1) / B;
         op.tiles = static_cast<unsigned>(static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1);
       };
       auto it = g_tune_cache.find(key);
@@ -880,12 +918,12 @@ void Plan::autotune() {
         dev::StageArgs T = A;
         T.in = s0;
         T.out = s1;
-        if (dev::launch_fft_fast(T, d_.dbl, op.inverse, A.load_afast != 0, op.tiles, st) != cudaSuccess) {
+        if (launch_fast_op(T, d_.dbl, op.kind, op.inverse, op.tiles, st) != cudaSuccess) {
           cudaGetLastError();
           continue;
         }
         cudaEventRecord(e0, st);
-        for (int r = 0; r < 3; ++r) dev::launch_fft_fast(T, d_.dbl, op.inverse, A.load_afast != 0, op.tiles, st);
+        for (int r = 0; r < 3; ++r) launch_fast_op(T, d_.dbl, op.kind, op.inverse, op.tiles, st);
         cudaEventRecord(e1, st);
         cuda_check(cudaEventSynchronize(e1), "tuner sync");
         float ms = 0.f;
@@ -924,7 +962,7 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
         A.in = buf(op0.src);
         A.out = buf(op0.dst);
         if (op0.fast)
-          e = dev::launch_fft_fast(A, d_.dbl, op0.inverse, A.load_afast != 0, op0.tiles, stream);
+          e = launch_fast_op(A, d_.dbl, op0.kind, op0.inverse, op0.tiles, stream);
         else
           e = dev::launch_fft_stage(A, d_.dbl, op0.kind, op0.inverse, op0.nthreads, op0.smem, op0.tiles, stream);
         break;

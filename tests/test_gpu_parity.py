@@ -225,3 +225,8 @@ def test_register_kernel_line_lengths(n, precision):
     for gin, axes, tin, tout in [((4, 6, n), (2,), (2, 1, 1), (1, 2, 1)), ((n, 3, 32), (0,), (1, 1, 2), (1, 1, 2)),
                                  ((n, 3, 32), (0,), (1, 2, 1), (1, 1, 2))]:
         check_roundtrip(gin, axes, tin, tout, False, precision=precision)
+    # R2C / C2R on contiguous lines (two real lines per register line); 15
+    # lines per block leave the last line of a pair empty
+    for gin, axes, tin, tout in [((4, 6, n), (2,), (2, 1, 1), (1, 2, 1)), ((3, 5, n), (2,), (1, 1, 1), (1, 1, 1)),
+                                 ((6, 4, n), (1, 2), (2, 1, 1), (1, 2, 1))]:
+        check_roundtrip(gin, axes, tin, tout, True, precision=precision)

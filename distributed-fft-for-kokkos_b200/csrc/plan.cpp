@@ -40,6 +40,7 @@ void cuda_check(cudaError_t e, const char* what) {
 // a power of two), then 3, 5, 7, 11, 13.
 std::vector<int> radix_plan(std::size_t n) {
   std::vector<int> r;
+  if (n == 0) fail(kErrInvalidExtents, "FFT length 0");
   std::size_t m = n;
   int k2 = 0;
   while (m % 2 == 0) {
@@ -338,8 +339,9 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   };
   std::size_t B = std::min<std::size_t>(d_.dbl ? 8 : 16, Dl.gext[b]);
   if (pairs && B > 1 && (B & 1)) ++B;
-  while (B > 1 && smem_for(B) > 100 * 1024) B = pairs ? std::max<std::size_t>(2, B - 2) : B - 1;
-  if (B == 2 && pairs && smem_for(B) > 100 * 1024) B = 2;
+  // shrink the tile to <= 100 KB of shared memory (pairs keep 2 lines)
+  const std::size_t Bmin = pairs ? 2 : 1;
+  while (B > Bmin && smem_for(B) > 100 * 1024) B = std::max(Bmin, B - (pairs ? 2 : 1));
   if (smem_for(B) > 227 * 1024) fail(kErrUnsupported, "FFT length " + std::to_string(n) + " too large for one stage");
   A.B = static_cast<int>(B);
   A.nl = static_cast<int>(pairs ? (B + 1) / 2 : B);

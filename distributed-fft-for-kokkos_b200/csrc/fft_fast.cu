@@ -1,9 +1,9 @@
 // Register-resident FFT stage for lines of 2^k or 3 * 2^k points (sm_100a).
 //
-// Used when both the source and the destination address every tile row as a
-// contiguous run: either every line is contiguous (unit stride along the FFT
-// axis a, "a-fast") or, for every position along a, the B lines of the tile
-// are contiguous (unit stride along the tile axis b, "b-fast").  Per-row base
+// Used when both the source and the destination have unit stride along the
+// FFT axis a ("a-fast": every line is one contiguous run) or along the tile
+// axis b ("b-fast": at every position along a, neighbouring lines of the tile
+// are neighbours in memory, except where a rank block ends).  Per-line base
 // offsets come from the separable layout tables, so the stage still performs
 // the reference's pack / all-to-all / unpack / local transpose by addressing.
 //
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r)];
     } else {
-      const C* col = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0) + line;
+      const C* col = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0 + line);
 #pragma unroll
       for (int q = 0; q < Q0; ++q)
 #pragma unroll
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
 #pragma unroll
         for (int r = 0; r < RL; ++r) row[out_pos<N, NPASS - 1, TT>(t, q, r)] = cscale(v[q * RL + r], s);
     } else {
-      C* col = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0) + line;
+      C* col = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0 + line);
 #pragma unroll
       for (int q = 0; q < QL; ++q)
 #pragma unroll

@@ -371,7 +371,10 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
     if (A.load_afast) {
       ok = contiguous(tables_[src_l], a, n, n) && contiguous(tables_[dst_l], a, n, n);
     } else {
-      ok = contiguous(tables_[src_l], b, Dl.gext[b], Bf) && contiguous(tables_[dst_l], b, Dl.gext[b], Bf);
+      // every line has its own base offset; unit stride along b (checked by
+      // layout_fast_axis) keeps the rows coalesced, rank-block ends only
+      // split them
+      ok = true;
     }
     if (ok) {
       op.fast = true;

@@ -170,6 +170,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="run only the FP32 warm-up and timed steps (for ncu captures); prints no bench line")
+    ap.add_argument("--profile-ns", type=int, default=0, metavar="EDGE",
+                    help="run only one FP32 Navier-Stokes RK4 step of a Taylor-Green field on EDGE^3 (for ncu "
+                         "captures); prints no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -207,6 +210,18 @@ def main():
     n = N_EDGE
     g = (n, n, n)
     stream = torch.cuda.current_stream()
+    if args.profile_ns:
+        e = args.profile_ns
+        pl = dfft.Plan((3, e, e, e), (3, e, e, e // 2 + 1), (1, 2, 3), (1, 2, 2, 1), (1, 1, 2, 2), real_input=True,
+                       precision="float32", stream=stream.cuda_stream)
+        st = dfft.NavierStokes(pl, nu=1.0 / 1600.0, dt=1e-3, lx=2.0)
+        uk = torch.empty(pl.buffer_elements("out"), dtype=torch.complex64, device="cuda")
+        st.init_taylor_green(uk, stream=stream.cuda_stream)
+        st.step(uk, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        print(f"profile run: Navier-Stokes {e}^3 energy {st.energy(uk, stream=stream.cuda_stream):.6f} "
+              "(not a bench value)", flush=True)
+        return
 
     def make(precision):
         return dfft.Plan(g, g, (0, 1, 2), TOPO_IN, TOPO_OUT, precision=precision, stream=stream.cuda_stream)

@@ -37,6 +37,9 @@ struct StageArgs {
   double scale;                 // applied on store
   int npass;
   unsigned long long radix_code;  // radix of pass p in bits [4p, 4p+4)
+  // register kernels: 1 = address each line as base + p * stride, both taken
+  // from the general layout tables (axis a lies inside one rank block)
+  int src_line_affine, dst_line_affine;
 };
 
 // Per-rank geometry of one transpose, packed as int64:

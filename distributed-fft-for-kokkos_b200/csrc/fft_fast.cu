@@ -243,6 +243,19 @@ __device__ __forceinline__ int64_t pick(const int64_t* a, int i) {
   return r;
 }
 
+// Base offset and stride along a of line (b = lb, o0 = c0, o1 = c1) of a
+// layout whose rank blocks do not split axis a.
+__device__ __forceinline__ void line_affine(const DevLayout& L, const StageArgs& A, int lb, int c0, int c1,
+                                            int64_t* base, int64_t* stride) {
+  int c[4] = {0, 0, 0, 0};
+  c[A.b] = lb;
+  if (A.o0 >= 0) c[A.o0] = c0;
+  if (A.o1 >= 0) c[A.o1] = c1;
+  *base = layout_offset(L, c, A.nd);
+  c[A.a] = 1;
+  *stride = layout_offset(L, c, A.nd) - *base;
+}
+
 }  // namespace
 
 // B lines per CTA, N/V threads per line.
@@ -288,19 +301,27 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
 
   // offsets shared by the whole tile (separable tables)
   int64_t so = 0, dof = 0;
-  if (A.o0 >= 0) {
-    so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
-    dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+  if (!A.src_line_affine) {
+    if (A.o0 >= 0) so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
+    if (A.o1 >= 0) so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
   }
-  if (A.o1 >= 0) {
-    so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
-    dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+  if (!A.dst_line_affine) {
+    if (A.o0 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+    if (A.o1 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
   }
 
   C v[V];
   constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
   const C* in = reinterpret_cast<const C*>(A.in);
-  if (active) {
+  if (active && A.src_line_affine) {
+    int64_t base, stride;
+    line_affine(ls, A, b0 + line, co0, co1, &base, &stride);
+    const C* row = in + base;
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r) * stride];
+  } else if (active) {
     if (AFAST) {
       const C* row = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0 + line) + __ldg(ls.t + pick(ls.off, A.a));
 #pragma unroll
@@ -325,7 +346,15 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
   constexpr int RL = Radix<N, NPASS - 1>::value, QL = V / RL;
   const T s = T(A.scale);
   C* out = reinterpret_cast<C*>(A.out);
-  if (active) {
+  if (active && A.dst_line_affine) {
+    int64_t base, stride;
+    line_affine(ld, A, b0 + line, co0, co1, &base, &stride);
+    C* row = out + base;
+#pragma unroll
+    for (int q = 0; q < QL; ++q)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) row[out_pos<N, NPASS - 1, TT>(t, q, r) * stride] = cscale(v[q * RL + r], s);
+  } else if (active) {
     if (AFAST) {
       C* row = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0 + line) + __ldg(ld.t + pick(ld.off, A.a));
 #pragma unroll
@@ -387,28 +416,37 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     const C* gtw = reinterpret_cast<const C*>(A.tw);
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   }
-  int64_t so = 0, dof = 0;
-  if (A.o0 >= 0) {
-    so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
-    dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+  // row bases (offset of position 0 of each real / complex line); lines are
+  // contiguous along a on both sides
+  int64_t srow0 = 0, srow1 = 0, drow0 = 0, drow1 = 0, unused;
+  if (A.src_line_affine) {
+    if (act0) line_affine(ls, A, b0 + r0, co0, co1, &srow0, &unused);
+    if (act1) line_affine(ls, A, b0 + r1, co0, co1, &srow1, &unused);
+  } else {
+    int64_t so = __ldg(ls.t + pick(ls.off, A.a));
+    if (A.o0 >= 0) so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
+    if (A.o1 >= 0) so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
+    srow0 = so + (act0 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r0) : 0);
+    srow1 = so + (act1 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r1) : 0);
   }
-  if (A.o1 >= 0) {
-    so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
-    dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+  if (A.dst_line_affine) {
+    if (act0) line_affine(ld, A, b0 + r0, co0, co1, &drow0, &unused);
+    if (act1) line_affine(ld, A, b0 + r1, co0, co1, &drow1, &unused);
+  } else {
+    int64_t dof = __ldg(ld.t + pick(ld.off, A.a));
+    if (A.o0 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+    if (A.o1 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+    drow0 = dof + (act0 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r0) : 0);
+    drow1 = dof + (act1 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r1) : 0);
   }
-  const int64_t sa0 = __ldg(ls.t + pick(ls.off, A.a)), da0 = __ldg(ld.t + pick(ld.off, A.a));
-  const int64_t sb0 = act0 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r0) : 0;
-  const int64_t sb1 = act1 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r1) : 0;
-  const int64_t db0 = act0 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r0) : 0;
-  const int64_t db1 = act1 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r1) : 0;
   const T s = T(A.scale);
 
   C v[V];
   constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
   if constexpr (!C2R) {
     const T* in = reinterpret_cast<const T*>(A.in);
-    const T* row0 = in + so + sb0 + sa0;
-    const T* row1 = in + so + sb1 + sa0;
+    const T* row0 = in + srow0;
+    const T* row1 = in + srow1;
 #pragma unroll
     for (int q = 0; q < Q0; ++q)
 #pragma unroll
@@ -419,8 +457,8 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     __syncthreads();  // twiddles staged
   } else {
     const C* in = reinterpret_cast<const C*>(A.in);
-    const C* row0 = in + so + sb0 + sa0;
-    const C* row1 = in + so + sb1 + sa0;
+    const C* row0 = in + srow0;
+    const C* row1 = in + srow1;
     for (int k = t; k <= H; k += TT) {
       const C x0 = act0 ? row0[k] : mk<T>(T(0), T(0));
       const C x1 = act1 ? row1[k] : mk<T>(T(0), T(0));
@@ -450,8 +488,8 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
       for (int r = 0; r < RL; ++r) ln[padpos<S>(out_pos<N, NPASS - 1, TT>(t, q, r))] = v[q * RL + r];
     __syncthreads();
     C* out = reinterpret_cast<C*>(A.out);
-    C* row0 = out + dof + db0 + da0;
-    C* row1 = out + dof + db1 + da0;
+    C* row0 = out + drow0;
+    C* row1 = out + drow1;
     const T hs = T(0.5) * s;
     for (int k = t; k <= H; k += TT) {
       const C z = ln[padpos<S>(k)];
@@ -464,8 +502,8 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     }
   } else {
     T* out = reinterpret_cast<T*>(A.out);
-    T* row0 = out + dof + db0 + da0;
-    T* row1 = out + dof + db1 + da0;
+    T* row0 = out + drow0;
+    T* row1 = out + drow1;
 #pragma unroll
     for (int q = 0; q < QL; ++q)
 #pragma unroll

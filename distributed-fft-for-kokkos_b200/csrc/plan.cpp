@@ -354,58 +354,51 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   op.nthreads = 256;
   if (!is_copy) A.tw = twiddle(n);
 
-  // Register-resident kernel: C2C power-of-two lines whose rows are
-  // contiguous runs on both sides (every line contiguous, or the B lines of
-  // a tile contiguous at every position along a).
-  if (kind == dev::kC2C && dev::fast_stage_supported(static_cast<int>(n)) && A.load_afast == A.store_afast &&
-      tables_[src_l].mode == 0 && tables_[dst_l].mode == 0 && S.gext[a] == n && Dl.gext[a] == n) {
-    const std::size_t Bf = static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)));
-    auto contiguous = [&](const LayoutTables& T, std::size_t axis, std::size_t len, std::size_t run) {
-      const std::int64_t* off = T.data.data() + T.off[axis];
-      for (std::size_t s0 = 0; s0 < len; s0 += run)
-        for (std::size_t c = s0 + 1; c < std::min(len, s0 + run); ++c)
-          if (off[c] != off[s0] + static_cast<std::int64_t>(c - s0)) return false;
-      return true;
-    };
-    bool ok;
-    if (A.load_afast) {
-      ok = contiguous(tables_[src_l], a, n, n) && contiguous(tables_[dst_l], a, n, n);
-    } else {
-      // every line has its own base offset; unit stride along b (checked by
-      // layout_fast_axis) keeps the rows coalesced, rank-block ends only
-      // split them
-      ok = true;
-    }
-    if (ok) {
-      op.fast = true;
-      A.B = static_cast<int>(Bf);
-      A.tiles_b = static_cast<int>((Dl.gext[b] + Bf - 1) / Bf);
-      const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
-      if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
-      op.tiles = static_cast<unsigned>(ft);
-    }
-  }
-  // Register-resident R2C (first) / C2R (last) stage: lines contiguous on
-  // both sides, every line a complete run of n reals / n/2+1 complex values.
-  if ((kind == dev::kR2C || kind == dev::kC2R) && dev::fast_stage_supported(static_cast<int>(n)) && A.load_afast &&
-      A.store_afast && tables_[src_l].mode == 0 && tables_[dst_l].mode == 0) {
-    const std::size_t nr = n, nc = n / 2 + 1;
-    const std::size_t ns = kind == dev::kR2C ? nr : nc, nd = kind == dev::kR2C ? nc : nr;
-    auto run_ok = [&](const LayoutTables& T, std::size_t len) {
+  // Register-resident kernels.  Each side of the stage either has separable
+  // tables (per-axis offset tables; lines read along a must then be one
+  // contiguous run) or general tables whose rank blocks do not split axis a
+  // (every line is affine, base + p * stride; lines read along a have unit
+  // stride because a is the layout's fast axis).
+  auto side_ok = [&](int l, const Layout& L, std::size_t len, bool afast, int* affine) {
+    const LayoutTables& T = tables_[l];
+    if (T.mode == 0) {
+      *affine = 0;
+      if (!afast) return true;
       const std::int64_t* off = T.data.data() + T.off[a];
       for (std::size_t c = 1; c < len; ++c)
         if (off[c] != off[0] + static_cast<std::int64_t>(c)) return false;
       return true;
-    };
-    if (S.gext[a] == ns && Dl.gext[a] == nd && run_ok(tables_[src_l], ns) && run_ok(tables_[dst_l], nd)) {
-      const std::size_t Bf = static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)));
-      op.fast = true;
-      A.B = static_cast<int>(Bf);
-      A.tiles_b = static_cast<int>((Dl.gext[b] + 2 * Bf - 1) / (2 * Bf));
-      const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
-      if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
-      op.tiles = static_cast<unsigned>(ft);
     }
+    *affine = 1;
+    return L.topo[a] == 1 && (!afast || layout_fast_axis(L) == a);
+  };
+  const std::size_t Bf = dev::fast_stage_supported(static_cast<int>(n))
+                             ? static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)))
+                             : 0;
+  int saff = 0, daff = 0;
+  // C2C: lines of n points on both sides, the same row orientation
+  if (kind == dev::kC2C && Bf && A.load_afast == A.store_afast && S.gext[a] == n && Dl.gext[a] == n &&
+      side_ok(src_l, S, n, A.load_afast != 0, &saff) && side_ok(dst_l, Dl, n, A.load_afast != 0, &daff)) {
+    op.fast = true;
+    A.B = static_cast<int>(Bf);
+    A.tiles_b = static_cast<int>((Dl.gext[b] + Bf - 1) / Bf);
+  }
+  // R2C (first) / C2R (last): lines of n reals and n/2+1 complex values, both
+  // read along a; two real lines per register line
+  const std::size_t nr = n, nc = n / 2 + 1;
+  const std::size_t ns = kind == dev::kR2C ? nr : nc, ndst = kind == dev::kR2C ? nc : nr;
+  if ((kind == dev::kR2C || kind == dev::kC2R) && Bf && A.load_afast && A.store_afast && S.gext[a] == ns &&
+      Dl.gext[a] == ndst && side_ok(src_l, S, ns, true, &saff) && side_ok(dst_l, Dl, ndst, true, &daff)) {
+    op.fast = true;
+    A.B = static_cast<int>(Bf);
+    A.tiles_b = static_cast<int>((Dl.gext[b] + 2 * Bf - 1) / (2 * Bf));
+  }
+  if (op.fast) {
+    A.src_line_affine = saff;
+    A.dst_line_affine = daff;
+    const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
+    if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
+    op.tiles = static_cast<unsigned>(ft);
   }
   return op;
 }

@@ -230,3 +230,16 @@ def test_register_kernel_line_lengths(n, precision):
     for gin, axes, tin, tout in [((4, 6, n), (2,), (2, 1, 1), (1, 2, 1)), ((3, 5, n), (2,), (1, 1, 1), (1, 1, 1)),
                                  ((6, 4, n), (1, 2), (2, 1, 1), (1, 2, 1))]:
         check_roundtrip(gin, axes, tin, tout, True, precision=precision)
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+@pytest.mark.parametrize("gin,axes,tin,tout,real", [
+    ((96, 64, 48), (0, 1, 2), (3, 2, 1), (1, 3, 2), True),     # out z = 25 over 2 ranks: 13 / 12
+    ((64, 96, 48), (0, 1, 2), (2, 2, 1), (1, 2, 2), True),
+    ((48, 40, 64), (0, 1, 2), (3, 1, 1), (1, 3, 1), False),    # y = 40 over 3 ranks: 14 / 13 / 13
+    ((3, 32, 24, 64), (1, 2, 3), (1, 3, 2, 1), (1, 1, 3, 2), True),
+])
+def test_register_kernels_on_ragged_blocks(gin, axes, tin, tout, real, precision):
+    # rank blocks of unequal size make the layout tables general (per-rank
+    # strides); the register kernels then address each line as base + p * stride
+    check_roundtrip(gin, axes, tin, tout, real, precision=precision)

@@ -259,7 +259,10 @@ __device__ __forceinline__ void line_affine(const DevLayout& L, const StageArgs&
 }  // namespace
 
 // B lines per CTA, N/V threads per line.
-template <typename T, bool INV, int N, int B, bool AFAST>
+// AFF: the general-layout variant (affine lines on the sides that set
+// src_line_affine / dst_line_affine); the separable variant carries none of
+// its code, which keeps its register count.
+template <typename T, bool INV, int N, int B, bool AFAST, bool AFF>
 __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const StageArgs A) {
   using C = cplx<T>;
   constexpr int V = Vals<N>::value;
@@ -301,19 +304,31 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
 
   // offsets shared by the whole tile (separable tables)
   int64_t so = 0, dof = 0;
-  if (!A.src_line_affine) {
-    if (A.o0 >= 0) so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
-    if (A.o1 >= 0) so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
-  }
-  if (!A.dst_line_affine) {
-    if (A.o0 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
-    if (A.o1 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+  const bool saff = AFF && A.src_line_affine, daff = AFF && A.dst_line_affine;
+  if constexpr (!AFF) {
+    if (A.o0 >= 0) {
+      so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
+      dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+    }
+    if (A.o1 >= 0) {
+      so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
+      dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+    }
+  } else {
+    if (!saff) {
+      if (A.o0 >= 0) so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
+      if (A.o1 >= 0) so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
+    }
+    if (!daff) {
+      if (A.o0 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+      if (A.o1 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+    }
   }
 
   C v[V];
   constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
   const C* in = reinterpret_cast<const C*>(A.in);
-  if (active && A.src_line_affine) {
+  if (AFF && active && saff) {
     int64_t base, stride;
     line_affine(ls, A, b0 + line, co0, co1, &base, &stride);
     const C* row = in + base;
@@ -346,7 +361,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
   constexpr int RL = Radix<N, NPASS - 1>::value, QL = V / RL;
   const T s = T(A.scale);
   C* out = reinterpret_cast<C*>(A.out);
-  if (active && A.dst_line_affine) {
+  if (AFF && active && daff) {
     int64_t base, stride;
     line_affine(ld, A, b0 + line, co0, co1, &base, &stride);
     C* row = out + base;
@@ -381,7 +396,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
 //   C2R: Z[k] = X0[k] + i X1[k] and Z[N-k] = conj X0[k] + i conj X1[k] are
 //        assembled in shared memory (imaginary parts of DC and Nyquist
 //        dropped), inverse FFT, x0 = Re z and x1 = Im z are written.
-template <typename T, bool C2R, int N, int B>
+template <typename T, bool C2R, int N, int B, bool AFF>
 __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const StageArgs A) {
   using C = cplx<T>;
   constexpr int V = Vals<N>::value;
@@ -419,7 +434,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
   // row bases (offset of position 0 of each real / complex line); lines are
   // contiguous along a on both sides
   int64_t srow0 = 0, srow1 = 0, drow0 = 0, drow1 = 0, unused;
-  if (A.src_line_affine) {
+  if (AFF && A.src_line_affine) {
     if (act0) line_affine(ls, A, b0 + r0, co0, co1, &srow0, &unused);
     if (act1) line_affine(ls, A, b0 + r1, co0, co1, &srow1, &unused);
   } else {
@@ -429,7 +444,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     srow0 = so + (act0 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r0) : 0);
     srow1 = so + (act1 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r1) : 0);
   }
-  if (A.dst_line_affine) {
+  if (AFF && A.dst_line_affine) {
     if (act0) line_affine(ld, A, b0 + r0, co0, co1, &drow0, &unused);
     if (act1) line_affine(ld, A, b0 + r1, co0, co1, &drow1, &unused);
   } else {
@@ -527,11 +542,11 @@ constexpr int fast_lines(int n) {
   return want < cap ? want : cap;
 }
 
-template <typename T, int N, bool INV, bool AF, int B>
+template <typename T, int N, bool INV, bool AF, int B, bool AFF = false>
 static cudaError_t launch_fast_b(const StageArgs& A, unsigned tiles, cudaStream_t st) {
   constexpr int LP = SmemShape<T, N, B, AF>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
-  auto k = fft_fast_kernel<T, INV, N, B, AF>;
+  auto k = fft_fast_kernel<T, INV, N, B, AF, AFF>;
   // raise the dynamic shared-memory limit once per kernel (not inside graph captures)
   static size_t attr_bytes = 48 * 1024;
   if (smem > attr_bytes) {
@@ -548,6 +563,8 @@ static cudaError_t launch_fast_n(const StageArgs& A, unsigned tiles, cudaStream_
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
+  if (A.src_line_affine || A.dst_line_affine)  // general layouts: default tile only
+    return A.B == B0 ? launch_fast_b<T, N, INV, AF, B0, true>(A, tiles, st) : cudaErrorInvalidValue;
   if (A.B == B0) return launch_fast_b<T, N, INV, AF, B0>(A, tiles, st);
   if (A.B == B1) return launch_fast_b<T, N, INV, AF, B1>(A, tiles, st);
   if (A.B == B2) return launch_fast_b<T, N, INV, AF, B2>(A, tiles, st);
@@ -562,11 +579,11 @@ static cudaError_t launch_fast_t(const StageArgs& A, bool inverse, bool afast, u
   return afast ? launch_fast_n<T, N, false, true>(A, tiles, st) : launch_fast_n<T, N, false, false>(A, tiles, st);
 }
 
-template <typename T, int N, bool C2R, int B>
+template <typename T, int N, bool C2R, int B, bool AFF = false>
 static cudaError_t launch_real_b(const StageArgs& A, unsigned tiles, cudaStream_t st) {
   constexpr int LP = SmemShape<T, N, B, true>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
-  auto k = fft_real_kernel<T, C2R, N, B>;
+  auto k = fft_real_kernel<T, C2R, N, B, AFF>;
   static size_t attr_bytes = 48 * 1024;
   if (smem > attr_bytes) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -582,6 +599,8 @@ static cudaError_t launch_real_n(const StageArgs& A, unsigned tiles, cudaStream_
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
+  if (A.src_line_affine || A.dst_line_affine)
+    return A.B == B0 ? launch_real_b<T, N, C2R, B0, true>(A, tiles, st) : cudaErrorInvalidValue;
   if (A.B == B0) return launch_real_b<T, N, C2R, B0>(A, tiles, st);
   if (A.B == B1) return launch_real_b<T, N, C2R, B1>(A, tiles, st);
   if (A.B == B2) return launch_real_b<T, N, C2R, B2>(A, tiles, st);

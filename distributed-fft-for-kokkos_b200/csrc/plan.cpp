@@ -883,6 +883,7 @@ void Plan::autotune() {
     for (auto& op : *progs) {
       if (op.type != Op::Stage || !op.fast) continue;
       dev::StageArgs& A = op.sa;
+      if (A.src_line_affine || A.dst_line_affine) continue;  // general layouts keep the default tile
       std::ostringstream k;
       const bool pairs = op.kind == dev::kR2C || op.kind == dev::kC2R;
       k << "fast:n" << A.n << (d_.dbl ? "f64" : "f32") << (op.inverse ? "i" : "f") << (A.load_afast ? "a" : "b")

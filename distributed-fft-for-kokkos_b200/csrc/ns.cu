@@ -40,6 +40,15 @@ __device__ __forceinline__ int64_t off4(const DevLayout& L, int d, int ix, int i
   return layout_offset(L, c, 4);
 }
 
+// offsets of the 3 components at (ix, iy, iz): the component axis is not
+// split across ranks, so they are o(0) + d * (o(1) - o(0))
+__device__ __forceinline__ void off3(const DevLayout& L, int ix, int iy, int iz, int64_t* o) {
+  o[0] = off4(L, 0, ix, iy, iz);
+  const int64_t step = off4(L, 1, ix, iy, iz) - o[0];
+  o[1] = o[0] + step;
+  o[2] = o[1] + step;
+}
+
 template <typename T>
 __global__ void ns_prep_kernel(const DevLayout L, cplx<T>* uk, cplx<T>* dx, cplx<T>* dy, cplx<T>* dz, NsGeom g) {
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
@@ -51,9 +60,11 @@ __global__ void ns_prep_kernel(const DevLayout L, cplx<T>* uk, cplx<T>* dx, cplx
     const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
     const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
     const T kx = T(mx * g.kscale), ky = T(my * g.kscale), kz = T(mz * g.kscale);
+    int64_t oc[3];
+    off3(L, ix, iy, iz, oc);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const int64_t o = off4(L, d, ix, iy, iz);
+      const int64_t o = oc[d];
       cplx<T> v = uk[o];
       if (!keep) v = mk<T>(T(0), T(0));
       uk[o] = v;
@@ -74,8 +85,7 @@ __global__ void ns_advection_kernel(const DevLayout L, T* u, const T* ux, const 
     const int iy = static_cast<int>((t / g.nz) % g.ny);
     const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nz) * g.ny));
     int64_t o[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) o[d] = off4(L, d, ix, iy, iz);
+    off3(L, ix, iy, iz, o);
     const T a = u[o[0]], b = u[o[1]], c = u[o[2]];
 #pragma unroll
     for (int d = 0; d < 3; ++d) u[o[d]] = a * ux[o[d]] + b * uy[o[d]] + c * uz[o[d]];
@@ -100,9 +110,9 @@ __global__ void ns_rhs_rk_kernel(const DevLayout L, cplx<T>* adv, cplx<T>* uk, c
     const T visc = T(-nu * ksq);
     int64_t o[3];
     cplx<T> r[3];
+    off3(L, ix, iy, iz, o);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      o[d] = off4(L, d, ix, iy, iz);
       cplx<T> a = adv[o[d]];
       if (!keep) a = mk<T>(T(0), T(0));
       const cplx<T> u = uk[o[d]];
@@ -156,9 +166,9 @@ __global__ void ns_project_kernel(const DevLayout L, cplx<T>* uk, NsGeom g) {
     const double inv_ksq = (ix == 0 && iy == 0 && iz == 0) ? 0.0 : 1.0 / (kx * kx + ky * ky + kz * kz);
     int64_t o[3];
     cplx<T> r[3];
+    off3(L, ix, iy, iz, o);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      o[d] = off4(L, d, ix, iy, iz);
       r[d] = keep ? uk[o[d]] : mk<T>(T(0), T(0));
     }
     const T ikk = T(inv_ksq);
@@ -180,9 +190,11 @@ __global__ void ns_taylor_green_kernel(const DevLayout L, T* u, NsGeom g, double
     const int iy = static_cast<int>((t / g.nz) % g.ny);
     const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nz) * g.ny));
     const double x = lx * pi * ix / g.nx, y = lx * pi * iy / g.ny, z = lx * pi * iz / g.nz;
-    u[off4(L, 0, ix, iy, iz)] = T(v0 * sin(x) * cos(y) * cos(z));
-    u[off4(L, 1, ix, iy, iz)] = T(-v0 * cos(x) * sin(y) * cos(z));
-    u[off4(L, 2, ix, iy, iz)] = T(0);
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
+    u[o[0]] = T(v0 * sin(x) * cos(y) * cos(z));
+    u[o[1]] = T(-v0 * cos(x) * sin(y) * cos(z));
+    u[o[2]] = T(0);
   }
 }
 
@@ -202,9 +214,11 @@ __global__ void ns_energy_kernel(const DevLayout L, const cplx<T>* uk, NsGeom g,
     const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
     const double factor = (iz == 0) ? 1.0 : 2.0;
     double e = 0.0;
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const cplx<T> v = uk[off4(L, d, ix, iy, iz)];
+      const cplx<T> v = uk[o[d]];
       e += double(v.x) * double(v.x) + double(v.y) * double(v.y);
     }
     acc += 0.5 * factor * e * coef;
@@ -254,9 +268,11 @@ void ck(cudaError_t e, const char* what) {
 
 NsState* ns_create(const Plan* plan, double nu, double dt, double lx) {
   const auto& d = plan->desc();
-  if (d.gin.size() != 4 || !d.r2c || d.axes != Ext{1, 2, 3} || d.gin[0] != 3 || !d.view_right)
+  if (d.gin.size() != 4 || !d.r2c || d.axes != Ext{1, 2, 3} || d.gin[0] != 3 || !d.view_right ||
+      d.in_topo[0] != 1 || d.out_topo[0] != 1)
     fail(kErrInvalidArgument,
-         "Navier-Stokes needs an R2C plan over LayoutRight 4D views (3, nx, ny, nz) with FFT axes {1, 2, 3}");
+         "Navier-Stokes needs an R2C plan over LayoutRight 4D views (3, nx, ny, nz) with FFT axes {1, 2, 3} and "
+         "the component axis not split (topology (1, px, py, 1) / (1, 1, px, py) as in the reference)");
   auto* s = new NsState;
   s->plan = plan;
   s->nu = nu;

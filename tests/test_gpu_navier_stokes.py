@@ -123,3 +123,7 @@ def test_ns_rejects_wrong_plan():
     plan = dfft.Plan((3, 16, 16, 16), (3, 16, 16, 16), (1, 2, 3), (1, 2, 1, 1), (1, 1, 2, 1))
     with pytest.raises(dfft.DistributedFFTError):
         dfft.NavierStokes(plan)
+    # component axis split across ranks
+    plan = dfft.Plan((3, 16, 16, 16), (3, 16, 16, 9), (1, 2, 3), (3, 1, 1, 1), (3, 1, 1, 1), real_input=True)
+    with pytest.raises(dfft.DistributedFFTError):
+        dfft.NavierStokes(plan)

@@ -377,6 +377,14 @@ dfft_status dfft_graph_create(dfft_graph** graph, const dfft_plan* const* plans,
         bidx[i] = static_cast<int>(it - ids.begin());
       }
     }
+    // a plan's transforms share its two scratch arrays: all of them must run
+    // in order on one branch
+    for (int64_t i = 0; i < count; ++i)
+      for (int64_t j = 0; j < i; ++j)
+        if (plans[i] == plans[j] && bidx[i] != bidx[j])
+          dfft::fail(dfft::kErrInvalidArgument,
+                     "a plan appears on two branches (items " + std::to_string(j) + " and " + std::to_string(i) +
+                         "): its transforms share the plan's scratch and must be on one branch");
     const std::size_t nb = ids.size();
     cudaStream_t cap = nullptr;
     ck(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream create");

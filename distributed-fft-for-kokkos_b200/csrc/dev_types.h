@@ -63,6 +63,12 @@ struct XposeArgs {
   void* dst;
 };
 
+// Raise `kernel`'s dynamic shared-memory limit to `smem` bytes on the current
+// device when a launch needs more than the default 48 KB there.  The attribute
+// belongs to the device, so it is recorded per (kernel, device), under a lock
+// (plans may be built and executed from several host threads).
+cudaError_t raise_smem_limit(const void* kernel, size_t smem);
+
 cudaError_t launch_fft_stage(const StageArgs& A, bool dbl, int kind, bool inverse, int nthreads, size_t smem,
                              unsigned tiles, cudaStream_t st);
 // Register-resident power-of-two stage (fft_fast.cu): line lengths 16..4096,

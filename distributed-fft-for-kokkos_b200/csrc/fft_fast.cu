@@ -547,13 +547,8 @@ static cudaError_t launch_fast_b(const StageArgs& A, unsigned tiles, cudaStream_
   constexpr int LP = SmemShape<T, N, B, AF>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
   auto k = fft_fast_kernel<T, INV, N, B, AF, AFF>;
-  // raise the dynamic shared-memory limit once per kernel (not inside graph captures)
-  static size_t attr_bytes = 48 * 1024;
-  if (smem > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    attr_bytes = smem;
-  }
+  const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
   k<<<tiles, N / Vals<N>::value * B, smem, st>>>(A);
   return cudaGetLastError();
 }
@@ -584,12 +579,8 @@ static cudaError_t launch_real_b(const StageArgs& A, unsigned tiles, cudaStream_
   constexpr int LP = SmemShape<T, N, B, true>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
   auto k = fft_real_kernel<T, C2R, N, B, AFF>;
-  static size_t attr_bytes = 48 * 1024;
-  if (smem > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    attr_bytes = smem;
-  }
+  const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
   k<<<tiles, N / Vals<N>::value * B, smem, st>>>(A);
   return cudaGetLastError();
 }

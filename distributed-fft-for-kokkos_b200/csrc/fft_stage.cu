@@ -13,6 +13,9 @@
 //               (this is where the reference's pack lands).
 // Twiddles come from a host table (long double, rounded to the stage
 // precision) staged in shared memory.
+#include <map>
+#include <mutex>
+
 #include "fft_stage.cuh"
 
 namespace dfft {
@@ -366,16 +369,25 @@ static cudaError_t launch_stage_t(const StageArgs& A, int kind, bool inverse, in
     case kCopyReal: k = fft_stage_kernel<T, kCopyReal, false>; break;
     default: return cudaErrorInvalidValue;
   }
-  // raise the dynamic shared-memory limit once per kernel (not inside graph captures)
-  static size_t attr_bytes[2 * 5] = {};
-  size_t& done = attr_bytes[kind * 2 + (inverse ? 1 : 0)];
-  if (smem > 48 * 1024 && smem > done) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    done = smem;
-  }
+  const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
   k<<<tiles, nthreads, smem, st>>>(A);
   return cudaGetLastError();
+}
+
+cudaError_t raise_smem_limit(const void* kernel, size_t smem) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> raised;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& done = raised[std::make_pair(kernel, dev)];
+  if (smem <= done) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess) done = smem;
+  return e;
 }
 
 cudaError_t launch_fft_stage(const StageArgs& A, bool dbl, int kind, bool inverse, int nthreads, size_t smem,

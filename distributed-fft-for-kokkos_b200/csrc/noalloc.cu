@@ -14,6 +14,9 @@
 //  * every extent a power of two in [16, 4096]; n0*n1*n2 complex elements of
 //    the chosen precision at most DFFT_NOALLOC_MAX_BYTES (64 MiB); anything
 //    else is rejected with DFFT_ERROR_UNSUPPORTED before any launch;
+//  * in and out must be aligned to one complex element (8 bytes for
+//    complex64, 16 for complex128); misaligned pointers are rejected with
+//    DFFT_ERROR_INVALID_ARGUMENT before any launch;
 //  * every GPU that loads the library holds the 64 MiB scratch (plus ~200 KB of
 //    tables and twiddles) until the process exits;
 //  * the first call on a device sets that device up (looks up the device
@@ -145,6 +148,14 @@ dfft_status dfft_noalloc_impl(const void* in, void* out, int64_t n0, int64_t n1,
     return DFFT_ERROR_UNSUPPORTED;
   }
   const bool dbl = precision == DFFT_PREC_F64;
+  // the stage kernels move whole complex elements (float2 / double2): a
+  // pointer off that alignment would fault on the device, so refuse it here
+  const uintptr_t align = dbl ? 16 : 8;
+  if (reinterpret_cast<uintptr_t>(in) % align != 0 || reinterpret_cast<uintptr_t>(out) % align != 0) {
+    *err = dbl ? "no-allocation FFT: in and out must be 16-byte aligned for complex128"
+               : "no-allocation FFT: in and out must be 8-byte aligned for complex64";
+    return DFFT_ERROR_INVALID_ARGUMENT;
+  }
   const unsigned long long bytes = static_cast<unsigned long long>(n0) * n1 * n2 * (dbl ? 16ull : 8ull);
   if (bytes > DFFT_NOALLOC_MAX_BYTES) {
     *err = "no-allocation FFT: the array exceeds the 64 MiB scratch (DFFT_NOALLOC_MAX_BYTES)";

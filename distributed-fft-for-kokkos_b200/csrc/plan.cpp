@@ -991,11 +991,27 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
   }
 }
 
+// The kernels move whole real / complex elements: a buffer off its element
+// alignment would fault on the device, so it is refused before any launch.
+void Plan::check_alignment(const void* p, bool complex, const char* which) const {
+  const std::uintptr_t real = d_.dbl ? 8 : 4;
+  const std::uintptr_t align = complex ? 2 * real : real;
+  if (reinterpret_cast<std::uintptr_t>(p) % align != 0)
+    fail(kErrInvalidArgument, std::string(which) + " buffer is not aligned to its element type (" +
+                                  std::to_string(align) + " bytes)");
+}
+
 void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream) const {
+  // forward: input layout -> complex output layout; backward: the reverse
+  check_alignment(in, forward ? lin_.complex : true, "input");
+  check_alignment(out, forward ? true : lin_.complex, "output");
   run_program(prog_[forward ? 0 : 1], in, out, stream);
 }
 
 void Plan::execute_adjoint(const void* in, void* out, bool of_forward, cudaStream_t stream) const {
+  // adjoint of forward: complex output layout -> input layout; of backward: the reverse
+  check_alignment(in, of_forward ? true : lin_.complex, "input");
+  check_alignment(out, of_forward ? lin_.complex : true, "output");
   run_program(adj_[of_forward ? 0 : 1], in, out, stream);
 }
 

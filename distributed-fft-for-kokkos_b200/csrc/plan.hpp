@@ -123,6 +123,7 @@ class Plan {
   void build_literal(bool forward);
   void build_adjoint(bool of_forward);
   void run_program(const std::vector<Op>& prog, const void* in, void* out, cudaStream_t stream) const;
+  void check_alignment(const void* p, bool complex, const char* which) const;
   void finalize_program(std::vector<Op>& prog, int cur_layout, int cur_buf, const Layout& final_layout,
                         double scale, bool final_complex);
   void allocate_device();

@@ -133,7 +133,9 @@ dfft_status dfft_plan_destroy(dfft_plan* plan);
  * blocks.  DFFT_FORWARD reads the input layout from `in` and writes the output
  * layout to `out`; DFFT_BACKWARD reads the (complex) output layout from `in`
  * and writes the input layout to `out`.  `in` is not modified.  Asynchronous
- * on the plan's stream. */
+ * on the plan's stream.  Each buffer must be aligned to its element type
+ * (real or complex of the plan's precision); a misaligned pointer is rejected
+ * with DFFT_ERROR_INVALID_ARGUMENT before any launch. */
 dfft_status dfft_execute(const dfft_plan* plan, const void* in, void* out, int32_t direction);
 
 /* Same as dfft_execute with an explicit stream (overrides the plan's). */
@@ -188,7 +190,9 @@ dfft_status dfft_get_topology_chain(const dfft_plan* plan, int64_t* n, uint64_t*
  * concurrently (branches = NULL: every transform on its own branch), so fields
  * of different sizes overlap.  The buffers are baked into the graph:
  * every dfft_graph_launch repeats the same transforms on the same pointers.
- * Plans must outlive the graph.  No counterpart in the reference (its
+ * Plans must outlive the graph.  All transforms of one plan must be on the
+ * same branch (they share the plan's scratch arrays); a plan on two branches
+ * is rejected with DFFT_ERROR_INVALID_ARGUMENT.  No counterpart in the reference (its
  * batched Navier-Stokes example loops over execute calls). */
 typedef struct dfft_graph_s dfft_graph;
 dfft_status dfft_graph_create(dfft_graph** graph, const dfft_plan* const* plans, const void* const* ins,
@@ -258,6 +262,8 @@ dfft_status dfft_get_workspace_bytes(const dfft_plan* plan, uint64_t* bytes);
  * that loads the library holds until the process exits.
  *   - every extent must be a power of two in [16, 4096] and the array at most
  *     DFFT_NOALLOC_MAX_BYTES; otherwise DFFT_ERROR_UNSUPPORTED;
+ *   - in and out must be aligned to one complex element (8 bytes for
+ *     complex64, 16 for complex128); otherwise DFFT_ERROR_INVALID_ARGUMENT;
  *   - the first call on a device sets the device up (synchronous copies of
  *     the twiddle tables): make it before any stream capture;
  *   - all calls share the library-owned arrays: calls that overlap on the GPU

@@ -82,4 +82,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_topology_tables.py <path to the reference checkout>")
+    main(sys.argv[1])

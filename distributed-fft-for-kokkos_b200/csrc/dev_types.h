@@ -40,6 +40,10 @@ struct StageArgs {
   // register kernels: 1 = address each line as base + p * stride, both taken
   // from the general layout tables (axis a lies inside one rank block)
   int src_line_affine, dst_line_affine;
+  // register kernels, separable sides: the offset table of axis a is affine,
+  // off_a[p] = abase + p * astride (checked on the host), so positions along
+  // the line are addressed without a table read
+  int64_t src_abase, dst_abase, src_astride, dst_astride;
 };
 
 // Per-rank geometry of one transpose, packed as int64:

@@ -167,6 +167,17 @@ __device__ __forceinline__ int out_pos(int t, int q, int r) {
   return (j - k) * R + k + r * Ns;
 }
 
+// Output position of value (q, r) of thread t after the last pass, minus t.
+// The earlier passes multiply to Ns = N / R_last and j = t + TT q < Ns, so the
+// Stockham index (j - j % Ns) R + j % Ns + r Ns reduces to j + r Ns: the
+// position is t plus a compile-time constant (no modulo by a 3 * 2^k Ns).
+template <int N, int TT>
+__device__ __forceinline__ constexpr int last_rel(int q, int r) {
+  constexpr int RL = Radix<N, Radix<N, 0>::npass - 1>::value;
+  static_assert(NsOf<N, Radix<N, 0>::npass - 1>::value * RL == N, "radix plan must multiply to N");
+  return TT * q + r * (N / RL);
+}
+
 template <typename T, bool INV, int N, int P, int TT>
 __device__ __forceinline__ void compute_pass(cplx<T>* v, int t, const cplx<T>* tw) {
   using C = cplx<T>;
@@ -262,8 +273,25 @@ __device__ __forceinline__ void line_affine(const DevLayout& L, const StageArgs&
 // AFF: the general-layout variant (affine lines on the sides that set
 // src_line_affine / dst_line_affine); the separable variant carries none of
 // its code, which keeps its register count.
+// Resident CTAs per SM the register budget is sized for.  Left alone, the
+// compiler gives the separable 8-value kernels a few registers more than the
+// budget of their natural occupancy (b-fast 1024-thread tiles lose half their
+// resident threads at 33+ registers), so they are held to 2048 (b-fast) or
+// 1536 (a-fast) complex64 threads, or 1024 complex128 threads, per SM.  The
+// other variants keep the compiler's choice (24-value threads cannot fit
+// those budgets).
+template <typename T, int N, int THREADS, bool AFAST, bool AFF>
+struct MinBlocks {
+  static constexpr bool bound = Vals<N>::value == 8 && !AFF;
+  static constexpr int target = sizeof(T) == 4 ? (AFAST ? 1536 : 2048) : 1024;
+  static constexpr int v = target / THREADS;
+  static constexpr int value = (bound && v > 0) ? v : 1;
+};
+
 template <typename T, bool INV, int N, int B, bool AFAST, bool AFF>
-__global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const StageArgs A) {
+__global__ void __launch_bounds__(N / Vals<N>::value * B,
+                                  (MinBlocks<T, N, N / Vals<N>::value * B, AFAST, AFF>::value))
+    fft_fast_kernel(const StageArgs A) {
   using C = cplx<T>;
   constexpr int V = Vals<N>::value;
   constexpr int TT = N / V;                  // threads per line
@@ -337,18 +365,20 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
 #pragma unroll
       for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r) * stride];
   } else if (active) {
+    const C* row = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0 + line) + A.src_abase;
     if (AFAST) {
-      const C* row = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0 + line) + __ldg(ls.t + pick(ls.off, A.a));
 #pragma unroll
       for (int q = 0; q < Q0; ++q)
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r)];
     } else {
-      const C* col = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0 + line);
+      // (N - 1) * stride < 2^31 (host check): 32-bit offsets along the line
+      const int st = static_cast<int>(A.src_astride);
+      row += static_cast<int64_t>(t) * st;
 #pragma unroll
       for (int q = 0; q < Q0; ++q)
 #pragma unroll
-        for (int r = 0; r < R0; ++r) v[q * R0 + r] = col[__ldg(ls.t + pick(ls.off, A.a) + in_pos<N, 0, TT>(t, q, r))];
+        for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[(TT * q + r * (N / R0)) * st];  // in_pos - t
     }
   } else {
 #pragma unroll
@@ -368,21 +398,21 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_fast_kernel(const 
 #pragma unroll
     for (int q = 0; q < QL; ++q)
 #pragma unroll
-      for (int r = 0; r < RL; ++r) row[out_pos<N, NPASS - 1, TT>(t, q, r) * stride] = cscale(v[q * RL + r], s);
+      for (int r = 0; r < RL; ++r) row[(t + last_rel<N, TT>(q, r)) * stride] = cscale(v[q * RL + r], s);
   } else if (active) {
+    C* row = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0 + line) + A.dst_abase;
     if (AFAST) {
-      C* row = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0 + line) + __ldg(ld.t + pick(ld.off, A.a));
 #pragma unroll
       for (int q = 0; q < QL; ++q)
 #pragma unroll
-        for (int r = 0; r < RL; ++r) row[out_pos<N, NPASS - 1, TT>(t, q, r)] = cscale(v[q * RL + r], s);
+        for (int r = 0; r < RL; ++r) row[t + last_rel<N, TT>(q, r)] = cscale(v[q * RL + r], s);
     } else {
-      C* col = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0 + line);
+      const int st = static_cast<int>(A.dst_astride);
+      row += static_cast<int64_t>(t) * st;
 #pragma unroll
       for (int q = 0; q < QL; ++q)
 #pragma unroll
-        for (int r = 0; r < RL; ++r)
-          col[__ldg(ld.t + pick(ld.off, A.a) + out_pos<N, NPASS - 1, TT>(t, q, r))] = cscale(v[q * RL + r], s);
+        for (int r = 0; r < RL; ++r) row[last_rel<N, TT>(q, r) * st] = cscale(v[q * RL + r], s);
     }
   }
 }
@@ -438,7 +468,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     if (act0) line_affine(ls, A, b0 + r0, co0, co1, &srow0, &unused);
     if (act1) line_affine(ls, A, b0 + r1, co0, co1, &srow1, &unused);
   } else {
-    int64_t so = __ldg(ls.t + pick(ls.off, A.a));
+    int64_t so = A.src_abase;
     if (A.o0 >= 0) so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
     if (A.o1 >= 0) so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
     srow0 = so + (act0 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r0) : 0);
@@ -448,7 +478,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     if (act0) line_affine(ld, A, b0 + r0, co0, co1, &drow0, &unused);
     if (act1) line_affine(ld, A, b0 + r1, co0, co1, &drow1, &unused);
   } else {
-    int64_t dof = __ldg(ld.t + pick(ld.off, A.a));
+    int64_t dof = A.dst_abase;
     if (A.o0 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
     if (A.o1 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
     drow0 = dof + (act0 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r0) : 0);
@@ -500,7 +530,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
 #pragma unroll
     for (int q = 0; q < QL; ++q)
 #pragma unroll
-      for (int r = 0; r < RL; ++r) ln[padpos<S>(out_pos<N, NPASS - 1, TT>(t, q, r))] = v[q * RL + r];
+      for (int r = 0; r < RL; ++r) ln[padpos<S>(t + last_rel<N, TT>(q, r))] = v[q * RL + r];
     __syncthreads();
     C* out = reinterpret_cast<C*>(A.out);
     C* row0 = out + drow0;
@@ -523,7 +553,7 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     for (int q = 0; q < QL; ++q)
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
-        const int p = out_pos<N, NPASS - 1, TT>(t, q, r);
+        const int p = t + last_rel<N, TT>(q, r);
         if (act0) row0[p] = v[q * RL + r].x * s;
         if (act1) row1[p] = v[q * RL + r].y * s;
       }

@@ -218,6 +218,9 @@ dfft_status dfft_noalloc_impl(const void* in, void* out, int64_t n0, int64_t n1,
     A.B = fast_stage_lines(dbl, A.n);
     A.tiles_b = (A.Eb + A.B - 1) / A.B;
     A.load_afast = A.store_afast = (a == 2) ? 1 : 0;
+    // C order: position p along axis a sits at p * (product of the faster extents)
+    A.src_abase = A.dst_abase = 0;
+    A.src_astride = A.dst_astride = (a == 0) ? n1 * n2 : (a == 1) ? n2 : 1;
     A.scale = si == 2 ? scale : 1.0;
     A.tw = dbl ? static_cast<const void*>(s->tw64 + tw_offset(A.n))
                : static_cast<const void*>(s->tw32 + tw_offset(A.n));

@@ -227,20 +227,31 @@ def all2all(sends, groups, layout_right=True):
 # ---------------------------------------------------------------------------
 # global transforms
 # ---------------------------------------------------------------------------
-def global_fft(x, axes, real_input, norm="backward"):
+def global_fft(x, axes, real_input, norm="backward", workers=None):
     """Global forward transform the reference's tests compare against
     (KokkosFFT::rfftn / fftn with the given normalisation; "none" scales by 1
-    in both directions)."""
+    in both directions).  FP64 pocketfft: numpy's, or scipy's (the same
+    library, multi-threaded) when `workers` is given for large grids."""
     x = np.asarray(x)
     npn = "backward" if norm == "none" else norm
+    if workers is not None:
+        import scipy.fft as sf
+        if real_input:
+            return sf.rfftn(x.astype(np.float64), axes=axes, norm=npn, workers=workers)
+        return sf.fftn(x.astype(np.complex128), axes=axes, norm=npn, workers=workers)
     if real_input:
         return np.fft.rfftn(x.astype(np.float64), axes=axes, norm=npn)
     return np.fft.fftn(x.astype(np.complex128), axes=axes, norm=npn)
 
 
-def global_ifft(X, axes, real_input, real_shape=None, norm="backward"):
+def global_ifft(X, axes, real_input, real_shape=None, norm="backward", workers=None):
     X = np.asarray(X).astype(np.complex128)
     npn = "forward" if norm == "none" else norm  # "forward" leaves the inverse unscaled
+    if workers is not None:
+        import scipy.fft as sf
+        if real_input:
+            return sf.irfftn(X, s=[real_shape[a] for a in axes], axes=axes, norm=npn, workers=workers)
+        return sf.ifftn(X, axes=axes, norm=npn, workers=workers)
     if real_input:
         s = [real_shape[a] for a in axes]
         return np.fft.irfftn(X, s=s, axes=axes, norm=npn)

@@ -193,6 +193,35 @@ def test_cfg2_pencil_c2c_256cubed(precision):
     assert O.rel_l2(xb, x) <= TOL[precision] * 2
 
 
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_headline_512cubed_pencil_c2c(precision):
+    """The bench workload itself: 512^3 C2C, pencil (4,4,1) -> (1,4,4), N(0,1)
+    complex from seed 1 (FP32 runs use the FP64 draws rounded).  Forward and
+    backward against the FP64 oracle on the same (rounded) inputs: rel-L2 <=
+    1e-12 in FP64, <= 1e-6 in FP32."""
+    gin = (512, 512, 512)
+    plan = dfft.Plan(gin, gin, (0, 1, 2), (4, 4, 1), (1, 4, 4), precision=precision)
+    x = random_input(gin, False, 1, precision)
+    X = run(plan, x, True)
+    ref = O.global_fft(x, (0, 1, 2), False, workers=-1)
+    e_fwd = O.rel_l2(X, ref)
+    del X
+    assert e_fwd <= TOL[precision], e_fwd
+    xb = run(plan, ref, False)  # backward of the exact spectrum
+    ref_b = x.astype(np.complex128)
+    e_bwd = O.rel_l2(xb, ref_b)
+    assert e_bwd <= TOL[precision], e_bwd
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_r2c_256cubed_pencil(precision):
+    """256^3 real U[-1,1) seed 1, R2C forward and C2R backward on the pencil
+    (4,4,1) -> (1,4,4), against the FP64 oracle."""
+    gin = (256, 256, 256)
+    plan, ef, eb = check_roundtrip(gin, (0, 1, 2), (4, 4, 1), (1, 4, 4), True, precision=precision, seed=1)
+    assert plan.name() == "PencilPlan"
+
+
 def test_cfg2_transposes_bit_exact_256cubed():
     gin = (256, 256, 256)
     plan = dfft.Plan(gin, gin, (0, 1, 2), (4, 4, 1), (1, 4, 4), exec_mode="literal_capture")

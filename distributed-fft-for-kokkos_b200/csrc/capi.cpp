@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/dfft.h"
+#include "exchange.hpp"
 #include "ns.hpp"
 #include "plan.hpp"
 
@@ -220,6 +221,23 @@ dfft_status dfft_get_num_blocks(const dfft_plan* plan, int64_t* nblocks) {
   });
 }
 
+static void fill_block_info(const dfft::BlockInfo& b, dfft_block_info* info) {
+  std::memset(info, 0, sizeof(*info));
+  info->block_type = b.block_type == dfft::BlockType::FFT ? 1 : 0;
+  info->block_idx = static_cast<int32_t>(b.block_idx);
+  info->fft_dim = static_cast<int32_t>(b.fft_dim);
+  info->in_axis = static_cast<int32_t>(b.in_axis);
+  info->out_axis = static_cast<int32_t>(b.out_axis);
+  info->comm_axis = static_cast<int32_t>(b.comm_axis);
+  copy_ext(b.in_topology, info->in_topology, DFFT_MAX_RANK);
+  copy_ext(b.out_topology, info->out_topology, DFFT_MAX_RANK);
+  copy_ext(b.in_extents, info->in_extents, DFFT_MAX_RANK);
+  copy_ext(b.out_extents, info->out_extents, DFFT_MAX_RANK);
+  copy_ext(b.buffer_extents, info->buffer_extents, DFFT_MAX_RANK + 1);
+  copy_ext(b.in_map, info->in_map, DFFT_MAX_RANK);
+  copy_ext(b.out_map, info->out_map, DFFT_MAX_RANK);
+}
+
 dfft_status dfft_get_block_info(const dfft_plan* plan, int64_t rank, int64_t block, dfft_block_info* info) {
   return guarded([&] {
     const auto& p = impl_of(plan);
@@ -229,21 +247,7 @@ dfft_status dfft_get_block_info(const dfft_plan* plan, int64_t rank, int64_t blo
     const auto& blocks = p.analyses().at(rank).blocks;
     if (block < 0 || static_cast<std::size_t>(block) >= blocks.size())
       dfft::fail(dfft::kErrInvalidArgument, "block index out of range");
-    const auto& b = blocks[block];
-    std::memset(info, 0, sizeof(*info));
-    info->block_type = b.block_type == dfft::BlockType::FFT ? 1 : 0;
-    info->block_idx = static_cast<int32_t>(b.block_idx);
-    info->fft_dim = static_cast<int32_t>(b.fft_dim);
-    info->in_axis = static_cast<int32_t>(b.in_axis);
-    info->out_axis = static_cast<int32_t>(b.out_axis);
-    info->comm_axis = static_cast<int32_t>(b.comm_axis);
-    copy_ext(b.in_topology, info->in_topology, DFFT_MAX_RANK);
-    copy_ext(b.out_topology, info->out_topology, DFFT_MAX_RANK);
-    copy_ext(b.in_extents, info->in_extents, DFFT_MAX_RANK);
-    copy_ext(b.out_extents, info->out_extents, DFFT_MAX_RANK);
-    copy_ext(b.buffer_extents, info->buffer_extents, DFFT_MAX_RANK + 1);
-    copy_ext(b.in_map, info->in_map, DFFT_MAX_RANK);
-    copy_ext(b.out_map, info->out_map, DFFT_MAX_RANK);
+    fill_block_info(blocks[block], info);
   });
 }
 
@@ -506,6 +510,214 @@ dfft_status dfft_ns_destroy(dfft_ns* ns) {
     if (!ns) return;
     dfft::ns_destroy(ns->impl);
     delete ns;
+  });
+}
+
+// ---- data-movement layer ----
+static dfft::Ext ext_of(const uint64_t* v, int32_t n, const char* what) {
+  if (!v) dfft::fail(dfft::kErrInvalidArgument, std::string("null ") + what);
+  if (n < 1 || n > DFFT_MAX_RANK + 1) dfft::fail(dfft::kErrInvalidArgument, std::string("bad rank of ") + what);
+  return dfft::Ext(v, v + n);
+}
+
+static dfft::Ext map_of(const int32_t* v, int32_t n, const char* what) {
+  if (!v) dfft::fail(dfft::kErrInvalidArgument, std::string("null ") + what);
+  dfft::Ext m;
+  for (int32_t i = 0; i < n; ++i) {
+    if (v[i] < 0 || v[i] >= n) dfft::fail(dfft::kErrInvalidArgument, std::string(what) + " entry out of range");
+    m.push_back(static_cast<std::size_t>(v[i]));
+  }
+  return m;
+}
+
+static void check_view_rank(int32_t rank) {
+  if (rank < 2 || rank > DFFT_MAX_RANK) dfft::fail(dfft::kErrInvalidArgument, "view rank must be in [2, 4]");
+}
+
+dfft_status dfft_pack(int32_t rank, const uint64_t* src_extents, const int32_t* src_map, int32_t axis,
+                      const uint64_t* buffer_extents, int32_t layout_right, int32_t element_bytes, const void* src,
+                      void* dst, void* stream) {
+  return guarded([&] {
+    check_view_rank(rank);
+    if (axis < 0 || axis >= rank) dfft::fail(dfft::kErrInvalidArgument, "axis out of range");
+    dfft::pack_local(ext_of(src_extents, rank, "src_extents"), map_of(src_map, rank, "src_map"),
+                     static_cast<std::size_t>(axis), ext_of(buffer_extents, rank + 1, "buffer_extents"),
+                     layout_right != 0, element_bytes, src, dst, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_unpack(int32_t rank, const uint64_t* buffer_extents, const int32_t* dst_map, int32_t axis,
+                        const uint64_t* dst_extents, int32_t layout_right, int32_t element_bytes, const void* src,
+                        void* dst, void* stream) {
+  return guarded([&] {
+    check_view_rank(rank);
+    if (axis < 0 || axis >= rank) dfft::fail(dfft::kErrInvalidArgument, "axis out of range");
+    dfft::unpack_local(ext_of(buffer_extents, rank + 1, "buffer_extents"), map_of(dst_map, rank, "dst_map"),
+                       static_cast<std::size_t>(axis), ext_of(dst_extents, rank, "dst_extents"), layout_right != 0,
+                       element_bytes, src, dst, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_all2all(int64_t nprocs, int32_t buffer_rank, const uint64_t* buffer_extents, int32_t layout_right,
+                         int32_t comm_axis, int32_t cart_rank, const uint64_t* cart_topology, int32_t element_bytes,
+                         const void* send, void* recv, void* stream) {
+  return guarded([&] {
+    if (nprocs <= 0) dfft::fail(dfft::kErrInvalidArgument, "nprocs must be positive");
+    dfft::Ext cart;
+    if (comm_axis >= 0) cart = ext_of(cart_topology, cart_rank, "cart_topology");
+    dfft::all2all_virtual(static_cast<std::size_t>(nprocs), ext_of(buffer_extents, buffer_rank, "buffer_extents"),
+                          layout_right != 0, cart, comm_axis, element_bytes, send, recv,
+                          static_cast<cudaStream_t>(stream));
+  });
+}
+
+struct dfft_trans_block_s {
+  dfft::TransBlockExec* impl;
+};
+
+dfft_status dfft_trans_block_create(dfft_trans_block** tb, const dfft_trans_block_desc* d) {
+  return guarded([&] {
+    if (!tb || !d) dfft::fail(dfft::kErrInvalidArgument, "null argument");
+    *tb = nullptr;
+    check_view_rank(d->rank);
+    const int32_t D = d->rank;
+    dfft::TransBlockDesc t;
+    t.gext = ext_of(d->global_extents, D, "global_extents");
+    t.in_topo = ext_of(d->in_topology, D, "in_topology");
+    t.out_topo = ext_of(d->out_topology, D, "out_topology");
+    t.in_right = d->in_topology_layout_right != 0;
+    t.out_right = d->out_topology_layout_right != 0;
+    t.src_map = map_of(d->src_map, D, "src_map");
+    t.dst_map = map_of(d->dst_map, D, "dst_map");
+    if (d->src_axis < 0 || d->src_axis >= D || d->dst_axis < 0 || d->dst_axis >= D)
+      dfft::fail(dfft::kErrInvalidArgument, "axis out of range");
+    t.src_axis = static_cast<std::size_t>(d->src_axis);
+    t.dst_axis = static_cast<std::size_t>(d->dst_axis);
+    t.view_right = d->view_layout_right != 0;
+    t.elem_bytes = d->element_bytes;
+    t.comm_axis = d->comm_axis;
+    bool any = false;
+    for (int32_t k = 0; k < D; ++k) any = any || d->cart_topology[k] != 0;
+    if (any) t.cart_topology = ext_of(d->cart_topology, D, "cart_topology");
+    auto* impl = new dfft::TransBlockExec(t);
+    *tb = new dfft_trans_block_s{impl};
+  });
+}
+
+static const dfft::TransBlockExec& tb_of(const dfft_trans_block* tb) {
+  if (!tb || !tb->impl) dfft::fail(dfft::kErrInvalidArgument, "null trans block");
+  return *tb->impl;
+}
+
+dfft_status dfft_trans_block_buffer_extents(const dfft_trans_block* tb, uint64_t* extents) {
+  return guarded([&] {
+    if (!extents) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    const auto& b = tb_of(tb).buffer_extents();
+    for (std::size_t k = 0; k < b.size(); ++k) extents[k] = b[k];
+  });
+}
+
+dfft_status dfft_trans_block_execute(const dfft_trans_block* tb, const void* in, void* out, void* send, void* recv,
+                                     int32_t direction, void* stream) {
+  return guarded([&] {
+    if (direction != DFFT_FORWARD && direction != DFFT_BACKWARD)
+      dfft::fail(dfft::kErrInvalidArgument, "Invalid FFT direction specified.");
+    tb_of(tb).execute(in, out, send, recv, direction == DFFT_FORWARD, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_trans_block_destroy(dfft_trans_block* tb) {
+  return guarded([&] {
+    if (!tb) return;
+    delete tb->impl;
+    delete tb;
+  });
+}
+
+// ---- layout math ----
+dfft_status dfft_rank_to_coord(int32_t rank, const uint64_t* topology, int32_t layout_right, int64_t rank_id,
+                               uint64_t* coord) {
+  return guarded([&] {
+    if (!coord) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    const dfft::Ext topo = ext_of(topology, rank, "topology");
+    if (rank_id < 0 || static_cast<std::size_t>(rank_id) >= dfft::total_size(topo))
+      dfft::fail(dfft::kErrInvalidArgument, "rank must be less than topology size.");
+    const dfft::Ext c = dfft::rank_to_coord(topo, static_cast<std::size_t>(rank_id), layout_right != 0);
+    for (std::size_t k = 0; k < c.size(); ++k) coord[k] = c[k];
+  });
+}
+
+dfft_status dfft_compute_local_extents_and_starts(int32_t rank, const uint64_t* global_extents,
+                                                  const uint64_t* topology, int32_t layout_right, int64_t rank_id,
+                                                  uint64_t* extents, uint64_t* starts) {
+  return guarded([&] {
+    if (!extents || !starts) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    const dfft::Ext g = ext_of(global_extents, rank, "global_extents"), topo = ext_of(topology, rank, "topology");
+    if (rank_id < 0 || static_cast<std::size_t>(rank_id) >= dfft::total_size(topo))
+      dfft::fail(dfft::kErrInvalidArgument, "rank must be less than topology size.");
+    const std::size_t r = static_cast<std::size_t>(rank_id);
+    const dfft::Ext e = dfft::compute_local_extents(g, topo, dfft::identity_map(g.size()), r, layout_right != 0);
+    const dfft::Ext st = dfft::compute_local_starts(g, topo, r, layout_right != 0);
+    for (std::size_t k = 0; k < g.size(); ++k) {
+      extents[k] = e[k];
+      starts[k] = st[k];
+    }
+  });
+}
+
+dfft_status dfft_compute_buffer_extents(int32_t rank, const uint64_t* global_extents, const uint64_t* in_topology,
+                                        const uint64_t* out_topology, int32_t layout_right,
+                                        uint64_t* buffer_extents) {
+  return guarded([&] {
+    if (!buffer_extents) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    const dfft::Ext b = dfft::compute_buffer_extents(ext_of(global_extents, rank, "global_extents"),
+                                                     ext_of(in_topology, rank, "in_topology"),
+                                                     ext_of(out_topology, rank, "out_topology"), layout_right != 0);
+    for (std::size_t k = 0; k < b.size(); ++k) buffer_extents[k] = b[k];
+  });
+}
+
+dfft_status dfft_permute_map_by_axes(int32_t rank, const int32_t* src_map, int32_t naxes, const int32_t* axes,
+                                     int32_t layout_right, int32_t* out_map) {
+  return guarded([&] {
+    if (!out_map) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    const dfft::Ext m = map_of(src_map, rank, "src_map");
+    dfft::Ext ax;
+    for (int32_t i = 0; i < naxes; ++i) {
+      if (!axes || axes[i] < 0 || axes[i] >= rank) dfft::fail(dfft::kErrInvalidArgument, "axes out of range");
+      ax.push_back(static_cast<std::size_t>(axes[i]));
+    }
+    const dfft::Ext r = dfft::permute_map_by_axes(m, ax, layout_right != 0);
+    for (std::size_t k = 0; k < r.size(); ++k) out_map[k] = static_cast<int32_t>(r[k]);
+  });
+}
+
+dfft_status dfft_propose_transpose_block(int32_t rank, const int32_t* map, const uint64_t* in_topology,
+                                         const uint64_t* out_topology, const uint64_t* in_extents,
+                                         const uint64_t* global_extents, int32_t naxes, const int32_t* axes,
+                                         int64_t rank_id, int32_t is_layout_right, int32_t is_last, int32_t in_axis,
+                                         int32_t out_axis, int32_t comm_axis, int64_t block_idx,
+                                         int64_t size_factor, int32_t view_layout_right, dfft_block_info* info,
+                                         uint64_t* max_buffer_size) {
+  return guarded([&] {
+    if (!info) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    check_view_rank(rank);
+    dfft::Ext ax;
+    for (int32_t i = 0; i < naxes; ++i) {
+      if (!axes || axes[i] < 0 || axes[i] >= rank) dfft::fail(dfft::kErrInvalidArgument, "axes out of range");
+      ax.push_back(static_cast<std::size_t>(axes[i]));
+    }
+    if (in_axis < 0 || out_axis < 0 || comm_axis < 0 || block_idx < 0 || size_factor < 0 || rank_id < 0)
+      dfft::fail(dfft::kErrInvalidArgument, "negative index");
+    std::size_t mb = 0;
+    const dfft::BlockInfo b = dfft::propose_transpose(
+        map_of(map, rank, "map"), ext_of(in_topology, rank, "in_topology"), ext_of(out_topology, rank, "out_topology"),
+        ext_of(in_extents, rank, "in_extents"), ext_of(global_extents, rank, "global_extents"), ax,
+        static_cast<std::size_t>(rank_id), is_layout_right != 0, is_last != 0, static_cast<std::size_t>(in_axis),
+        static_cast<std::size_t>(out_axis), static_cast<std::size_t>(comm_axis), static_cast<std::size_t>(block_idx),
+        static_cast<std::size_t>(size_factor), view_layout_right != 0, &mb);
+    fill_block_info(b, info);
+    if (max_buffer_size) *max_buffer_size = mb;
   });
 }
 

@@ -19,6 +19,8 @@
 //             for bit-exact comparison with the reference's buffers.
 #include "plan.hpp"
 
+#include "exchange.hpp"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -359,14 +361,22 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   // contiguous run) or general tables whose rank blocks do not split axis a
   // (every line is affine, base + p * stride; lines read along a have unit
   // stride because a is the layout's fast axis).
-  auto side_ok = [&](int l, const Layout& L, std::size_t len, bool afast, int* affine) {
+  auto side_ok = [&](int l, const Layout& L, std::size_t len, bool afast, int* affine, std::int64_t* abase,
+                     std::int64_t* astride) {
     const LayoutTables& T = tables_[l];
     if (T.mode == 0) {
+      // separable: the offsets along a must be affine (unit stride when the
+      // lines are read along a)
       *affine = 0;
-      if (!afast) return true;
       const std::int64_t* off = T.data.data() + T.off[a];
+      const std::int64_t st = len > 1 ? off[1] - off[0] : 1;
+      if (afast && st != 1) return false;
       for (std::size_t c = 1; c < len; ++c)
-        if (off[c] != off[0] + static_cast<std::int64_t>(c)) return false;
+        if (off[c] != off[0] + static_cast<std::int64_t>(c) * st) return false;
+      // the kernels take 32-bit offsets along a line
+      if (static_cast<std::int64_t>(len - 1) * (st < 0 ? -st : st) >= (std::int64_t(1) << 31)) return false;
+      *abase = off[0];
+      *astride = st;
       return true;
     }
     *affine = 1;
@@ -376,9 +386,11 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
                              ? static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)))
                              : 0;
   int saff = 0, daff = 0;
+  std::int64_t sab = 0, sas = 0, dab = 0, das = 0;
   // C2C: lines of n points on both sides, the same row orientation
   if (kind == dev::kC2C && Bf && A.load_afast == A.store_afast && S.gext[a] == n && Dl.gext[a] == n &&
-      side_ok(src_l, S, n, A.load_afast != 0, &saff) && side_ok(dst_l, Dl, n, A.load_afast != 0, &daff)) {
+      side_ok(src_l, S, n, A.load_afast != 0, &saff, &sab, &sas) &&
+      side_ok(dst_l, Dl, n, A.load_afast != 0, &daff, &dab, &das)) {
     op.fast = true;
     A.B = static_cast<int>(Bf);
     A.tiles_b = static_cast<int>((Dl.gext[b] + Bf - 1) / Bf);
@@ -388,7 +400,8 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   const std::size_t nr = n, nc = n / 2 + 1;
   const std::size_t ns = kind == dev::kR2C ? nr : nc, ndst = kind == dev::kR2C ? nc : nr;
   if ((kind == dev::kR2C || kind == dev::kC2R) && Bf && A.load_afast && A.store_afast && S.gext[a] == ns &&
-      Dl.gext[a] == ndst && side_ok(src_l, S, ns, true, &saff) && side_ok(dst_l, Dl, ndst, true, &daff)) {
+      Dl.gext[a] == ndst && side_ok(src_l, S, ns, true, &saff, &sab, &sas) &&
+      side_ok(dst_l, Dl, ndst, true, &daff, &dab, &das)) {
     op.fast = true;
     A.B = static_cast<int>(Bf);
     A.tiles_b = static_cast<int>((Dl.gext[b] + 2 * Bf - 1) / (2 * Bf));
@@ -396,6 +409,10 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   if (op.fast) {
     A.src_line_affine = saff;
     A.dst_line_affine = daff;
+    A.src_abase = sab;
+    A.src_astride = sas;
+    A.dst_abase = dab;
+    A.dst_astride = das;
     const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
     if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
     op.tiles = static_cast<unsigned>(ft);
@@ -525,42 +542,13 @@ void Plan::build_adjoint(bool of_forward) {
 // Literal program (reference block sequence)
 // ---------------------------------------------------------------------------
 std::int64_t Plan::add_geo(const Layout& L, const BlockInfo& b, std::size_t pc) {
-  const std::size_t P = nprocs();
-  auto blocks = layout_blocks(L);
   // Exchange groups: the whole communicator for slabs; for pencils the row /
   // column communicators of MPI_Cart_create over the non-one entries of the
   // input topology (reorder = 0, row-major) split by MPI_Cart_sub
   // (KokkosFFT_Distributed_PencilPlan.hpp:32-71), picked by comm_axis.
-  std::vector<std::size_t> dims;
-  for (auto t : d_.in_topo)
-    if (t > 1) dims.push_back(t);
   const std::int64_t base = static_cast<std::int64_t>(host_tables_.size());
-  for (std::size_t r = 0; r < P; ++r) {
-    for (int k = 0; k < 4; ++k)
-      host_tables_.push_back(k < static_cast<int>(L.gext.size()) ? static_cast<std::int64_t>(blocks[r].starts[k]) : 0);
-    for (int k = 0; k < 4; ++k)
-      host_tables_.push_back(k < static_cast<int>(L.gext.size()) ? static_cast<std::int64_t>(blocks[r].local[k]) : 0);
-    std::size_t sub = r;
-    std::vector<std::size_t> members(pc);
-    if (type_ == TopologyType::Pencil) {
-      const std::size_t t1 = dims.at(1);
-      const std::size_t c0 = r / t1, c1 = r % t1;
-      if (b.comm_axis == 0) {
-        if (pc != dims.at(0)) fail(kErrInternal, "row communicator size mismatch");
-        sub = c0;
-        for (std::size_t j = 0; j < pc; ++j) members[j] = j * t1 + c1;
-      } else {
-        if (pc != t1) fail(kErrInternal, "column communicator size mismatch");
-        sub = c1;
-        for (std::size_t j = 0; j < pc; ++j) members[j] = c0 * t1 + j;
-      }
-    } else {
-      if (pc != P) fail(kErrInternal, "communicator size mismatch");
-      for (std::size_t j = 0; j < pc; ++j) members[j] = j;
-    }
-    host_tables_.push_back(static_cast<std::int64_t>(sub));
-    for (auto m : members) host_tables_.push_back(static_cast<std::int64_t>(m));
-  }
+  append_exchange_geo(host_tables_, L, d_.in_topo, type_ == TopologyType::Pencil ? static_cast<int>(b.comm_axis) : -1,
+                      pc);
   return base;
 }
 

@@ -748,6 +748,18 @@ std::vector<Proposal> propose_block(const ProposeContext& c, const std::vector<B
 
 }  // namespace
 
+BlockInfo propose_transpose(const Ext& map, const Ext& in_topo, const Ext& out_topo, const Ext& in_extents,
+                            const Ext& global_extents, const Ext& axes, std::size_t rank, bool is_layout_right,
+                            bool is_last, std::size_t in_axis, std::size_t out_axis, std::size_t comm_axis,
+                            std::size_t block_idx, std::size_t size_factor, bool view_layout_right,
+                            std::size_t* max_buffer_size) {
+  const Proposal p = propose_transpose_block(map, in_topo, out_topo, in_extents, global_extents, axes, rank,
+                                             is_layout_right, is_last, in_axis, out_axis, comm_axis, block_idx,
+                                             size_factor, view_layout_right);
+  if (max_buffer_size) *max_buffer_size = p.max_buffer_size;
+  return p.block;
+}
+
 BlockAnalyses slab_block_analyses(const Ext& in_extents, const Ext& gin, const Ext& gout, const Ext& in_topo,
                                   const Ext& out_topo, const Ext& axes, bool real_input, bool view_layout_right,
                                   std::size_t rank) {

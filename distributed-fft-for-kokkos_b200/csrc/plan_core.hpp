@@ -130,6 +130,14 @@ BlockAnalyses pencil_block_analyses(const Ext& in_extents, const Ext& gin, const
                                     bool in_right, const Ext& out_topo, bool out_right, const Ext& axes,
                                     bool real_input, bool view_layout_right, std::size_t rank);
 
+// propose_transpose_block (KokkosFFT_Distributed_BlockAnalyses.hpp:93-136):
+// one transpose block and its max buffer size (elements of the real type).
+BlockInfo propose_transpose(const Ext& map, const Ext& in_topo, const Ext& out_topo, const Ext& in_extents,
+                            const Ext& global_extents, const Ext& axes, std::size_t rank, bool is_layout_right,
+                            bool is_last, std::size_t in_axis, std::size_t out_axis, std::size_t comm_axis,
+                            std::size_t block_idx, std::size_t size_factor, bool view_layout_right,
+                            std::size_t* max_buffer_size);
+
 // Validation of the global extents for a transform (are_valid_extents,
 // KokkosFFT_Distributed_MPI_Extents.hpp:322-417).  `real_input` selects R2C.
 void check_valid_extents(const Ext& gin, const Ext& gout, const Ext& axes, bool real_input,

@@ -51,6 +51,28 @@ class BlockInfo(ctypes.Structure):
     ]
 
 
+class TransBlockDesc(ctypes.Structure):
+    _fields_ = [
+        ("rank", ctypes.c_int32),
+        ("global_extents", ctypes.c_uint64 * MAX_RANK),
+        ("in_topology", ctypes.c_uint64 * MAX_RANK),
+        ("out_topology", ctypes.c_uint64 * MAX_RANK),
+        ("in_topology_layout_right", ctypes.c_int32),
+        ("out_topology_layout_right", ctypes.c_int32),
+        ("src_map", ctypes.c_int32 * MAX_RANK),
+        ("dst_map", ctypes.c_int32 * MAX_RANK),
+        ("src_axis", ctypes.c_int32),
+        ("dst_axis", ctypes.c_int32),
+        ("view_layout_right", ctypes.c_int32),
+        ("element_bytes", ctypes.c_int32),
+        ("comm_axis", ctypes.c_int32),
+        ("cart_topology", ctypes.c_uint64 * MAX_RANK),
+    ]
+
+
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+_I32P = ctypes.POINTER(ctypes.c_int32)
+
 # name -> (restype, argtypes); the complete list of entry points of dfft.h
 SIGNATURES = {
     "dfft_plan_desc_init": (None, [ctypes.POINTER(PlanDesc)]),
@@ -106,6 +128,31 @@ SIGNATURES = {
     "dfft_ns_energy": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     "dfft_ns_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dfft_pack": (
+        ctypes.c_int, [ctypes.c_int32, _U64P, _I32P, ctypes.c_int32, _U64P, ctypes.c_int32, ctypes.c_int32,
+                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_unpack": (
+        ctypes.c_int, [ctypes.c_int32, _U64P, _I32P, ctypes.c_int32, _U64P, ctypes.c_int32, ctypes.c_int32,
+                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_all2all": (
+        ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, _U64P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _U64P,
+                       ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_trans_block_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(TransBlockDesc)]),
+    "dfft_trans_block_buffer_extents": (ctypes.c_int, [ctypes.c_void_p, _U64P]),
+    "dfft_trans_block_execute": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.c_int32, ctypes.c_void_p]),
+    "dfft_trans_block_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dfft_rank_to_coord": (ctypes.c_int, [ctypes.c_int32, _U64P, ctypes.c_int32, ctypes.c_int64, _U64P]),
+    "dfft_compute_local_extents_and_starts": (
+        ctypes.c_int, [ctypes.c_int32, _U64P, _U64P, ctypes.c_int32, ctypes.c_int64, _U64P, _U64P]),
+    "dfft_compute_buffer_extents": (ctypes.c_int, [ctypes.c_int32, _U64P, _U64P, _U64P, ctypes.c_int32, _U64P]),
+    "dfft_permute_map_by_axes": (
+        ctypes.c_int, [ctypes.c_int32, _I32P, ctypes.c_int32, _I32P, ctypes.c_int32, _I32P]),
+    "dfft_propose_transpose_block": (
+        ctypes.c_int, [ctypes.c_int32, _I32P, _U64P, _U64P, _U64P, _U64P, ctypes.c_int32, _I32P, ctypes.c_int64,
+                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64,
+                       ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(BlockInfo), _U64P]),
     "dfft_last_error_string": (ctypes.c_char_p, []),
     "dfft_version": (ctypes.c_char_p, []),
 }

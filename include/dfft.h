@@ -232,6 +232,102 @@ dfft_status dfft_get_all_topologies(int32_t pencil, int32_t rank, const uint64_t
                                     int32_t fft_rank, const int32_t* axes, int64_t* n, uint64_t* topologies,
                                     int64_t* trans_axes, int64_t* layouts);
 
+/* ---- The data-movement layer on its own ----
+ * The reference's pack / unpack of one rank's view
+ * (KokkosFFT::Distributed::Impl::pack / unpack,
+ * KokkosFFT_Distributed_PackUnpack.hpp:439-499), its all-to-all
+ * (Impl::all2all, KokkosFFT_Distributed_MPI_All2All.hpp:23-58) here over every
+ * virtual rank at once, and the TransBlock that chains them
+ * (KokkosFFT_Distributed_TransBlock.hpp:38-107).  They run the same kernels as
+ * the plans' literal programs.
+ *   - views and buffers are device arrays of elements of element_bytes (4, 8
+ *     or 16; the kernels copy whole elements, so float, double, complex64 and
+ *     complex128 all work) aligned to element_bytes;
+ *   - a view of rank D gives its extents in its own dimension order (the
+ *     rank's local extents permuted by its map: dimension i holds logical
+ *     axis map[i]); a buffer has rank D + 1, the process dimension first for
+ *     layout_right = 1 (LayoutRight) and last for 0 (LayoutLeft), which is
+ *     also the memory order of views and buffers;
+ *   - pack splits logical axis `axis` into the buffer's process bins (the
+ *     first n % P bins one larger, zeros outside a bin); unpack merges it;
+ *   - asynchronous on `stream`; pack / unpack / all2all use a few hundred
+ *     bytes of stream-ordered device memory for their index tables. */
+dfft_status dfft_pack(int32_t rank, const uint64_t* src_extents, const int32_t* src_map, int32_t axis,
+                      const uint64_t* buffer_extents, int32_t layout_right, int32_t element_bytes, const void* src,
+                      void* dst, void* stream);
+dfft_status dfft_unpack(int32_t rank, const uint64_t* buffer_extents, const int32_t* dst_map, int32_t axis,
+                        const uint64_t* dst_extents, int32_t layout_right, int32_t element_bytes, const void* src,
+                        void* dst, void* stream);
+/* MPI_Alltoall of every virtual rank: send and recv hold nprocs buffers of
+ * buffer_extents (rank buffer_rank), rank after rank; recv of rank r, chunk j
+ * = send of the j-th member of r's communicator, chunk (r's rank in it).
+ * comm_axis -1: one communicator of all ranks; 0 / 1: the row / column
+ * communicators MPI_Cart_sub keeps from MPI_Cart_create over the entries of
+ * cart_topology (cart_rank entries) larger than one (row-major, no
+ * reordering), as the pencil plans build them
+ * (KokkosFFT_Distributed_PencilPlan.hpp:32-71).  The buffer's process extent
+ * must equal the communicator size. */
+dfft_status dfft_all2all(int64_t nprocs, int32_t buffer_rank, const uint64_t* buffer_extents, int32_t layout_right,
+                         int32_t comm_axis, int32_t cart_rank, const uint64_t* cart_topology, int32_t element_bytes,
+                         const void* send, void* recv, void* stream);
+
+/* TransBlock over every rank of a topology pair.  Forward packs the input
+ * blocks (in_topology, src_map) along src_axis, exchanges, and unpacks into
+ * the output blocks (out_topology, dst_map) merging dst_axis; backward is the
+ * reverse.  The buffer extents are compute_buffer_extents(global_extents,
+ * in_topology, out_topology) (dfft_trans_block_buffer_extents). */
+typedef struct {
+  int32_t rank;                           /* view rank, 2..4 */
+  uint64_t global_extents[DFFT_MAX_RANK];
+  uint64_t in_topology[DFFT_MAX_RANK];
+  uint64_t out_topology[DFFT_MAX_RANK];
+  int32_t in_topology_layout_right;       /* rank order of in_topology (1 LayoutRight) */
+  int32_t out_topology_layout_right;
+  int32_t src_map[DFFT_MAX_RANK];         /* map of the input views */
+  int32_t dst_map[DFFT_MAX_RANK];         /* map of the output views */
+  int32_t src_axis;                       /* forward: split on send */
+  int32_t dst_axis;                       /* forward: merged on receive */
+  int32_t view_layout_right;              /* memory order of views and buffers */
+  int32_t element_bytes;                  /* 4, 8 or 16 */
+  int32_t comm_axis;                      /* as dfft_all2all */
+  uint64_t cart_topology[DFFT_MAX_RANK];  /* as dfft_all2all; all zeros: in_topology */
+} dfft_trans_block_desc;
+typedef struct dfft_trans_block_s dfft_trans_block;
+dfft_status dfft_trans_block_create(dfft_trans_block** tb, const dfft_trans_block_desc* desc);
+/* rank + 1 entries */
+dfft_status dfft_trans_block_buffer_extents(const dfft_trans_block* tb, uint64_t* extents);
+/* in / out: every rank's block concatenated in rank order; send / recv: nprocs
+ * buffers.  Views and buffers must not alias (TransBlock::good). */
+dfft_status dfft_trans_block_execute(const dfft_trans_block* tb, const void* in, void* out, void* send, void* recv,
+                                     int32_t direction, void* stream);
+dfft_status dfft_trans_block_destroy(dfft_trans_block* tb);
+
+/* ---- Layout math on the host (no GPU) ----
+ * rank_to_coord (KokkosFFT_Distributed_MPI_Extents.hpp:492-529). */
+dfft_status dfft_rank_to_coord(int32_t rank, const uint64_t* topology, int32_t layout_right, int64_t rank_id,
+                               uint64_t* coord);
+/* compute_local_extents_and_starts of one rank (MPI_Extents.hpp:546-577). */
+dfft_status dfft_compute_local_extents_and_starts(int32_t rank, const uint64_t* global_extents,
+                                                  const uint64_t* topology, int32_t layout_right, int64_t rank_id,
+                                                  uint64_t* extents, uint64_t* starts);
+/* compute_buffer_extents<Layout> (KokkosFFT_Distributed_Extents.hpp:35-90):
+ * rank + 1 entries. */
+dfft_status dfft_compute_buffer_extents(int32_t rank, const uint64_t* global_extents, const uint64_t* in_topology,
+                                        const uint64_t* out_topology, int32_t layout_right,
+                                        uint64_t* buffer_extents);
+/* permute_map_by_axes<Layout> (KokkosFFT_Distributed_Mapping.hpp:39-110). */
+dfft_status dfft_permute_map_by_axes(int32_t rank, const int32_t* src_map, int32_t naxes, const int32_t* axes,
+                                     int32_t layout_right, int32_t* out_map);
+/* propose_transpose_block (KokkosFFT_Distributed_BlockAnalyses.hpp:93-136):
+ * the block of rank `rank_id` and its max buffer size. */
+dfft_status dfft_propose_transpose_block(int32_t rank, const int32_t* map, const uint64_t* in_topology,
+                                         const uint64_t* out_topology, const uint64_t* in_extents,
+                                         const uint64_t* global_extents, int32_t naxes, const int32_t* axes,
+                                         int64_t rank_id, int32_t is_layout_right, int32_t is_last, int32_t in_axis,
+                                         int32_t out_axis, int32_t comm_axis, int64_t block_idx,
+                                         int64_t size_factor, int32_t view_layout_right, dfft_block_info* info,
+                                         uint64_t* max_buffer_size);
+
 /* Copy data recorded by the last DFFT_EXEC_LITERAL_CAPTURE execution in
  * `direction` for transpose block `block` (index in the block list) to host:
  *   which = 0 send buffers, 1 recv buffers: nprocs x prod(buffer_extents)

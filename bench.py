@@ -18,7 +18,8 @@ Reported:
   roofline   the FFT stage kernel (every launch of the step) against the
              measured HBM copy bandwidth
   cpu_baseline  the CPU oracle (numpy restatement of the reference block walk)
-             on a bounded 256^3 sample, rank 0 only
+             on a bounded 256^3 sample of the same pencil, all host threads,
+             rank 0 only
 
 ``--impl reference`` times the CPU restatement of the reference's execute
 path (the reference itself cannot be built here: Kokkos, kokkos-fft, FFTW and
@@ -107,19 +108,32 @@ def stop_clock_sampler(p, path):
             "samples": len(sm)}
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(steps=2, workers=None):
-    """CPU oracle on a bounded sample (256^3 complex64, same topology)."""
+    """CPU oracle (numpy restatement of the reference's block walk: pocketfft
+    local FFTs on `workers` threads, pack / all-to-all / unpack) on a bounded
+    sample of the workload: the same pencil at 256^3.  The block list comes
+    from oracle/plans/ (precomputed planner output), so this leg loads no
+    product code."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
     import numpy as np
 
-    import dfft
     import dfft_oracle as O
-    from _plan_info import plan_info
 
     n = CPU_SAMPLE_EDGE
-    p = dfft.Plan((n,) * 3, (n,) * 3, (0, 1, 2), TOPO_IN, TOPO_OUT, precision="float32", analyze_only=True)
-    info = plan_info(p)
+    with open(os.path.join(ROOT, "oracle", "plans", f"c2c_{n}_pencil_441_144.json")) as f:
+        info = json.load(f)["plan"]
+    workers = workers or os.cpu_count() or 1
     rng = np.random.default_rng(1)
     x = (rng.standard_normal((n,) * 3) + 1j * rng.standard_normal((n,) * 3)).astype(np.complex64)
     t0 = time.perf_counter()
@@ -128,10 +142,18 @@ def cpu_baseline(steps=2, workers=None):
         O.execute_literal(y, info, False, workers=workers)
     dt = (time.perf_counter() - t0) / steps
     return {
-        "value": round(algo_bytes(n, 8) / dt / 1e9, 3), "unit": "GB/s", "cores": workers or 1, "kind": "port",
-        "ms_per_step": round(dt * 1e3, 1),
-        "sample": f"{n}^3 C2C complex64 fwd+bwd, pencil {TOPO_IN}->{TOPO_OUT}, numpy restatement of the "
-                  f"reference block walk (pocketfft local FFTs, pack/all2all/unpack), {steps} steps"}
+        "value": round(algo_bytes(n, 8) / dt / 1e9, 3), "unit": "GB/s", "cores": workers, "kind": "port",
+        "cpu_model": cpu_model(), "ms_per_step": round(dt * 1e3, 1),
+        "sample": f"{n}^3 C2C complex64 fwd+bwd on the same pencil {TOPO_IN}->{TOPO_OUT} (a bounded sample of the "
+                  f"{N_EDGE}^3 workload, same GB/s metric), numpy restatement of the reference block walk (pocketfft "
+                  f"local FFTs on {workers} threads, pack/all2all/unpack), {steps} steps"}
+
+
+def workload_config(world):
+    return {"workload": WORKLOAD, "n": N_EDGE, "topology_in": list(TOPO_IN), "topology_out": list(TOPO_OUT),
+            "precision": "complex64", "exec_mode": "fused", "graph": True,
+            "l2": "inputs (1 GiB per field) larger than the 126 MB L2",
+            "parallelism": f"weak, one {N_EDGE}^3 field per GPU x {world}"}
 
 
 def run_reference(args):
@@ -151,10 +173,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": N_EDGE, "topology_in": list(TOPO_IN), "topology_out": list(TOPO_OUT),
-                   "precision": "complex64",
-                   "sample": f"each step is a bounded {CPU_SAMPLE_EDGE}^3 sample of the workload on the host CPU "
-                             "(CPU restatement of the reference execute path)"},
+        "config": workload_config(args.gpus),
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -441,13 +460,11 @@ def main():
     per_launch_bytes = step_bytes / launches
     launch_ms = ms32 / launches
     achieved = per_launch_bytes / (launch_ms * 1e-3) / 1e9
-    traffic = None  # dram bytes per launch from the committed full ncu capture of this workload
+    traffic = None  # dram bytes per launch from the committed ncu capture of this workload
     try:
-        with open(os.path.join(ROOT, "profiles", "fft_fast_kernel_512cubed_c64_full.md")) as f:
-            for ln in f:
-                if ln.startswith("traffic_per_launch_bytes:"):
-                    traffic = int(ln.split(":")[1])
-    except Exception:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            traffic = int(json.load(f)["fft_fast_kernel_512cubed_c64"]["traffic_per_launch_bytes"])
+    except (OSError, KeyError, ValueError):
         pass
 
     if rank == 0:
@@ -455,10 +472,7 @@ def main():
             "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms32, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (complex N(0,1), torch generator seed 1234+rank)",
-            "config": {"workload": WORKLOAD, "n": n, "topology_in": list(TOPO_IN), "topology_out": list(TOPO_OUT),
-                       "precision": "complex64", "exec_mode": "fused", "graph": True,
-                       "l2": "inputs (1 GiB per field) larger than the 126 MB L2",
-                       "parallelism": f"weak, one 512^3 field per GPU x {world}"},
+            "config": workload_config(world),
             "gflops": round(world * flops(n) / (ms32 * 1e-3) / 1e9, 1),
             "execution": "CUDA graph of forward + backward (plan-time autotuned kernels)",
             "eager_ms_per_step": round(ms32_eager, 4),
@@ -482,7 +496,7 @@ def main():
             "gpu_launches": int(launches * args.steps),
         }
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(steps=2)
+            line["cpu_baseline"] = cpu_baseline(steps=2, workers=os.cpu_count())
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -44,6 +44,10 @@ struct StageArgs {
   // off_a[p] = abase + p * astride (checked on the host), so positions along
   // the line are addressed without a table read
   int64_t src_abase, dst_abase, src_astride, dst_astride;
+  // register kernels, separable sides: start of the offset tables of axes a,
+  // b, o0, o1 in src.t / dst.t (filled by the launcher from src.off /
+  // dst.off, so the kernels select no table at run time)
+  int64_t s_ta, s_tb, s_to0, s_to1, d_ta, d_tb, d_to0, d_to1;
 };
 
 // Per-rank geometry of one transpose, packed as int64:
@@ -84,9 +88,11 @@ int fast_stage_line_options(bool dbl, int n, int* opts);
 // R2C first stage (c2r = false) or C2R last stage (c2r = true) of the
 // register-resident kernel; lines contiguous on both sides; A.B complex lines
 // (2 A.B real lines) per tile
-cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, unsigned tiles, cudaStream_t st);
-cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, unsigned tiles,
-                            cudaStream_t st);
+// The register kernels run a grid of (tiles_b, Eo0, Eo1) CTAs; Eo0 and Eo1
+// must be at most fast_stage_max_grid_yz().
+cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, cudaStream_t st);
+cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, cudaStream_t st);
+constexpr int fast_stage_max_grid_yz() { return 65535; }
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
 cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);

@@ -245,15 +245,6 @@ __device__ __forceinline__ void run_fft(cplx<T>* v, int t, const cplx<T>* tw, cp
   }
 }
 
-// a[i] without a runtime-indexed (local-memory) array access
-__device__ __forceinline__ int64_t pick(const int64_t* a, int i) {
-  int64_t r = a[0];
-#pragma unroll
-  for (int k = 1; k < 4; ++k)
-    if (i == k) r = a[k];
-  return r;
-}
-
 // Base offset and stride along a of line (b = lb, o0 = c0, o1 = c1) of a
 // layout whose rank blocks do not split axis a.
 __device__ __forceinline__ void line_affine(const DevLayout& L, const StageArgs& A, int lb, int c0, int c1,
@@ -274,16 +265,19 @@ __device__ __forceinline__ void line_affine(const DevLayout& L, const StageArgs&
 // src_line_affine / dst_line_affine); the separable variant carries none of
 // its code, which keeps its register count.
 // Resident CTAs per SM the register budget is sized for.  Left alone, the
-// compiler gives the separable 8-value kernels a few registers more than the
-// budget of their natural occupancy (b-fast 1024-thread tiles lose half their
-// resident threads at 33+ registers), so they are held to 2048 (b-fast) or
-// 1536 (a-fast) complex64 threads, or 1024 complex128 threads, per SM.  The
-// other variants keep the compiler's choice (24-value threads cannot fit
-// those budgets).
+// compiler spends registers on scheduling freedom: the separable 8-value
+// kernels take a few more than the budget of their natural occupancy (b-fast
+// 1024-thread tiles lose half their resident threads at 33+ registers) and
+// the 24-value kernels anything up to 150.  So 8-value kernels are held to
+// 2048 (b-fast) or 1536 (a-fast) complex64 threads, or 1024 complex128
+// threads, per SM, and 24-value kernels to 768 complex64 or 384 complex128
+// threads (about 85 / 170 registers).  The general-layout 8-value variant
+// keeps the compiler's choice.
 template <typename T, int N, int THREADS, bool AFAST, bool AFF>
 struct MinBlocks {
-  static constexpr bool bound = Vals<N>::value == 8 && !AFF;
-  static constexpr int target = sizeof(T) == 4 ? (AFAST ? 1536 : 2048) : 1024;
+  static constexpr bool v8 = Vals<N>::value == 8;
+  static constexpr bool bound = !(v8 && AFF);
+  static constexpr int target = v8 ? (sizeof(T) == 4 ? (AFAST ? 1536 : 2048) : 1024) : (sizeof(T) == 4 ? 768 : 384);
   static constexpr int v = target / THREADS;
   static constexpr int value = (bound && v > 0) ? v : 1;
 };
@@ -303,14 +297,8 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B,
   C* tile = tw + N;
   const DevLayout ls = A.src, ld = A.dst;
 
-  int tb = blockIdx.x % A.tiles_b;
-  int rest = blockIdx.x / A.tiles_b;
-  int co0 = 0, co1 = 0;
-  if (A.o0 >= 0) {
-    co0 = rest % A.Eo0;
-    rest /= A.Eo0;
-  }
-  if (A.o1 >= 0) co1 = rest;
+  // grid (tiles_b, Eo0, Eo1): tile along b, coordinates along o0 and o1
+  const int tb = blockIdx.x, co0 = blockIdx.y, co1 = blockIdx.z;
   const int b0 = tb * B;
   const int nb = min(B, A.Eb - b0);
 
@@ -335,50 +323,64 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B,
   const bool saff = AFF && A.src_line_affine, daff = AFF && A.dst_line_affine;
   if constexpr (!AFF) {
     if (A.o0 >= 0) {
-      so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
-      dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
+      so += __ldg(ls.t + A.s_to0 + co0);
+      dof += __ldg(ld.t + A.d_to0 + co0);
     }
     if (A.o1 >= 0) {
-      so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
-      dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+      so += __ldg(ls.t + A.s_to1 + co1);
+      dof += __ldg(ld.t + A.d_to1 + co1);
     }
   } else {
     if (!saff) {
-      if (A.o0 >= 0) so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
-      if (A.o1 >= 0) so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
+      if (A.o0 >= 0) so += __ldg(ls.t + A.s_to0 + co0);
+      if (A.o1 >= 0) so += __ldg(ls.t + A.s_to1 + co1);
     }
     if (!daff) {
-      if (A.o0 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
-      if (A.o1 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
+      if (A.o0 >= 0) dof += __ldg(ld.t + A.d_to0 + co0);
+      if (A.o1 >= 0) dof += __ldg(ld.t + A.d_to1 + co1);
     }
   }
 
   C v[V];
   constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
   const C* in = reinterpret_cast<const C*>(A.in);
-  if (AFF && active && saff) {
-    int64_t base, stride;
-    line_affine(ls, A, b0 + line, co0, co1, &base, &stride);
-    const C* row = in + base;
+  if (active) {
+    if constexpr (AFF) {
+      // general-layout variant: each side is one affine line, base + p * stride
+      int64_t base, stride;
+      if (saff) {
+        line_affine(ls, A, b0 + line, co0, co1, &base, &stride);
+      } else {
+        base = so + __ldg(ls.t + A.s_tb + b0 + line) + A.src_abase;
+        stride = A.src_astride;
+      }
+      const C* row = in + base;
 #pragma unroll
-    for (int q = 0; q < Q0; ++q)
+      for (int q = 0; q < Q0; ++q)
 #pragma unroll
-      for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r) * stride];
-  } else if (active) {
-    const C* row = in + so + __ldg(ls.t + pick(ls.off, A.b) + b0 + line) + A.src_abase;
-    if (AFAST) {
+        for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r) * stride];
+    } else if (AFAST) {
+      const C* row = in + so + __ldg(ls.t + A.s_tb + b0 + line) + A.src_abase;
 #pragma unroll
       for (int q = 0; q < Q0; ++q)
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r)];
-    } else {
+    } else if constexpr (V == 8) {
       // (N - 1) * stride < 2^31 (host check): 32-bit offsets along the line
       const int st = static_cast<int>(A.src_astride);
-      row += static_cast<int64_t>(t) * st;
+      const C* row = in + so + __ldg(ls.t + A.s_tb + b0 + line) + A.src_abase + static_cast<int64_t>(t) * st;
 #pragma unroll
       for (int q = 0; q < Q0; ++q)
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[(TT * q + r * (N / R0)) * st];  // in_pos - t
+    } else {
+      // 24 values a thread: offsets read from the axis table one at a time
+      // keep fewer addresses live than 24 precomputed products
+      const C* col = in + so + __ldg(ls.t + A.s_tb + b0 + line);
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[q * R0 + r] = col[__ldg(ls.t + A.s_ta + in_pos<N, 0, TT>(t, q, r))];
     }
   } else {
 #pragma unroll
@@ -389,30 +391,45 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B,
   run_fft<T, INV, N, 0, TT, SH::S>(v, t, tw, tile + line * LP);
 
   constexpr int RL = Radix<N, NPASS - 1>::value, QL = V / RL;
-  const T s = T(A.scale);
+  if (A.scale != 1.0) {  // only the normalised direction's last stage scales
+    const T s = T(A.scale);
+#pragma unroll
+    for (int e = 0; e < V; ++e) v[e] = cscale(v[e], s);
+  }
   C* out = reinterpret_cast<C*>(A.out);
-  if (AFF && active && daff) {
-    int64_t base, stride;
-    line_affine(ld, A, b0 + line, co0, co1, &base, &stride);
-    C* row = out + base;
-#pragma unroll
-    for (int q = 0; q < QL; ++q)
-#pragma unroll
-      for (int r = 0; r < RL; ++r) row[(t + last_rel<N, TT>(q, r)) * stride] = cscale(v[q * RL + r], s);
-  } else if (active) {
-    C* row = out + dof + __ldg(ld.t + pick(ld.off, A.b) + b0 + line) + A.dst_abase;
-    if (AFAST) {
+  if (active) {
+    if constexpr (AFF) {
+      int64_t base, stride;
+      if (daff) {
+        line_affine(ld, A, b0 + line, co0, co1, &base, &stride);
+      } else {
+        base = dof + __ldg(ld.t + A.d_tb + b0 + line) + A.dst_abase;
+        stride = A.dst_astride;
+      }
+      C* row = out + base;
 #pragma unroll
       for (int q = 0; q < QL; ++q)
 #pragma unroll
-        for (int r = 0; r < RL; ++r) row[t + last_rel<N, TT>(q, r)] = cscale(v[q * RL + r], s);
-    } else {
+        for (int r = 0; r < RL; ++r) row[(t + last_rel<N, TT>(q, r)) * stride] = v[q * RL + r];
+    } else if (AFAST) {
+      C* row = out + dof + __ldg(ld.t + A.d_tb + b0 + line) + A.dst_abase;
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) row[t + last_rel<N, TT>(q, r)] = v[q * RL + r];
+    } else if constexpr (V == 8) {
       const int st = static_cast<int>(A.dst_astride);
-      row += static_cast<int64_t>(t) * st;
+      C* row = out + dof + __ldg(ld.t + A.d_tb + b0 + line) + A.dst_abase + static_cast<int64_t>(t) * st;
 #pragma unroll
       for (int q = 0; q < QL; ++q)
 #pragma unroll
-        for (int r = 0; r < RL; ++r) row[last_rel<N, TT>(q, r) * st] = cscale(v[q * RL + r], s);
+        for (int r = 0; r < RL; ++r) row[last_rel<N, TT>(q, r) * st] = v[q * RL + r];
+    } else {
+      C* col = out + dof + __ldg(ld.t + A.d_tb + b0 + line);
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) col[__ldg(ld.t + A.d_ta + t + last_rel<N, TT>(q, r))] = v[q * RL + r];
     }
   }
 }
@@ -441,14 +458,8 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
   C* tile = tw + N;
   const DevLayout ls = A.src, ld = A.dst;
 
-  int tb = blockIdx.x % A.tiles_b;
-  int rest = blockIdx.x / A.tiles_b;
-  int co0 = 0, co1 = 0;
-  if (A.o0 >= 0) {
-    co0 = rest % A.Eo0;
-    rest /= A.Eo0;
-  }
-  if (A.o1 >= 0) co1 = rest;
+  // grid (tiles_b, Eo0, Eo1): tile along b, coordinates along o0 and o1
+  const int tb = blockIdx.x, co0 = blockIdx.y, co1 = blockIdx.z;
   const int b0 = tb * 2 * B;               // first real line of the tile
   const int nbr = min(2 * B, A.Eb - b0);   // real lines in the tile
   const int t = threadIdx.x % TT;
@@ -469,20 +480,20 @@ __global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const 
     if (act1) line_affine(ls, A, b0 + r1, co0, co1, &srow1, &unused);
   } else {
     int64_t so = A.src_abase;
-    if (A.o0 >= 0) so += __ldg(ls.t + pick(ls.off, A.o0) + co0);
-    if (A.o1 >= 0) so += __ldg(ls.t + pick(ls.off, A.o1) + co1);
-    srow0 = so + (act0 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r0) : 0);
-    srow1 = so + (act1 ? __ldg(ls.t + pick(ls.off, A.b) + b0 + r1) : 0);
+    if (A.o0 >= 0) so += __ldg(ls.t + A.s_to0 + co0);
+    if (A.o1 >= 0) so += __ldg(ls.t + A.s_to1 + co1);
+    srow0 = so + (act0 ? __ldg(ls.t + A.s_tb + b0 + r0) : 0);
+    srow1 = so + (act1 ? __ldg(ls.t + A.s_tb + b0 + r1) : 0);
   }
   if (AFF && A.dst_line_affine) {
     if (act0) line_affine(ld, A, b0 + r0, co0, co1, &drow0, &unused);
     if (act1) line_affine(ld, A, b0 + r1, co0, co1, &drow1, &unused);
   } else {
     int64_t dof = A.dst_abase;
-    if (A.o0 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o0) + co0);
-    if (A.o1 >= 0) dof += __ldg(ld.t + pick(ld.off, A.o1) + co1);
-    drow0 = dof + (act0 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r0) : 0);
-    drow1 = dof + (act1 ? __ldg(ld.t + pick(ld.off, A.b) + b0 + r1) : 0);
+    if (A.o0 >= 0) dof += __ldg(ld.t + A.d_to0 + co0);
+    if (A.o1 >= 0) dof += __ldg(ld.t + A.d_to1 + co1);
+    drow0 = dof + (act0 ? __ldg(ld.t + A.d_tb + b0 + r0) : 0);
+    drow1 = dof + (act1 ? __ldg(ld.t + A.d_tb + b0 + r1) : 0);
   }
   const T s = T(A.scale);
 
@@ -572,59 +583,77 @@ constexpr int fast_lines(int n) {
   return want < cap ? want : cap;
 }
 
+// Grid of a stage and the table offsets the kernels read (host side).
+static dim3 fast_grid(const StageArgs& A) {
+  return dim3(static_cast<unsigned>(A.tiles_b), static_cast<unsigned>(A.Eo0), static_cast<unsigned>(A.Eo1));
+}
+
+static StageArgs with_table_offsets(const StageArgs& A) {
+  StageArgs R = A;
+  R.s_ta = A.src.off[A.a];
+  R.d_ta = A.dst.off[A.a];
+  R.s_tb = A.src.off[A.b];
+  R.d_tb = A.dst.off[A.b];
+  R.s_to0 = A.o0 >= 0 ? A.src.off[A.o0] : 0;
+  R.d_to0 = A.o0 >= 0 ? A.dst.off[A.o0] : 0;
+  R.s_to1 = A.o1 >= 0 ? A.src.off[A.o1] : 0;
+  R.d_to1 = A.o1 >= 0 ? A.dst.off[A.o1] : 0;
+  return R;
+}
+
 template <typename T, int N, bool INV, bool AF, int B, bool AFF = false>
-static cudaError_t launch_fast_b(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+static cudaError_t launch_fast_b(const StageArgs& A, cudaStream_t st) {
   constexpr int LP = SmemShape<T, N, B, AF>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
   auto k = fft_fast_kernel<T, INV, N, B, AF, AFF>;
   const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
   if (e != cudaSuccess) return e;
-  k<<<tiles, N / Vals<N>::value * B, smem, st>>>(A);
+  k<<<fast_grid(A), N / Vals<N>::value * B, smem, st>>>(with_table_offsets(A));
   return cudaGetLastError();
 }
 
 template <typename T, int N, bool INV, bool AF>
-static cudaError_t launch_fast_n(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+static cudaError_t launch_fast_n(const StageArgs& A, cudaStream_t st) {
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
   if (A.src_line_affine || A.dst_line_affine)  // general layouts: default tile only
-    return A.B == B0 ? launch_fast_b<T, N, INV, AF, B0, true>(A, tiles, st) : cudaErrorInvalidValue;
-  if (A.B == B0) return launch_fast_b<T, N, INV, AF, B0>(A, tiles, st);
-  if (A.B == B1) return launch_fast_b<T, N, INV, AF, B1>(A, tiles, st);
-  if (A.B == B2) return launch_fast_b<T, N, INV, AF, B2>(A, tiles, st);
+    return A.B == B0 ? launch_fast_b<T, N, INV, AF, B0, true>(A, st) : cudaErrorInvalidValue;
+  if (A.B == B0) return launch_fast_b<T, N, INV, AF, B0>(A, st);
+  if (A.B == B1) return launch_fast_b<T, N, INV, AF, B1>(A, st);
+  if (A.B == B2) return launch_fast_b<T, N, INV, AF, B2>(A, st);
   return cudaErrorInvalidValue;
 }
 
 template <typename T, int N>
-static cudaError_t launch_fast_t(const StageArgs& A, bool inverse, bool afast, unsigned tiles, cudaStream_t st) {
+static cudaError_t launch_fast_t(const StageArgs& A, bool inverse, bool afast, cudaStream_t st) {
   if (inverse) {
-    return afast ? launch_fast_n<T, N, true, true>(A, tiles, st) : launch_fast_n<T, N, true, false>(A, tiles, st);
+    return afast ? launch_fast_n<T, N, true, true>(A, st) : launch_fast_n<T, N, true, false>(A, st);
   }
-  return afast ? launch_fast_n<T, N, false, true>(A, tiles, st) : launch_fast_n<T, N, false, false>(A, tiles, st);
+  return afast ? launch_fast_n<T, N, false, true>(A, st) : launch_fast_n<T, N, false, false>(A, st);
 }
 
 template <typename T, int N, bool C2R, int B, bool AFF = false>
-static cudaError_t launch_real_b(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+static cudaError_t launch_real_b(const StageArgs& A, cudaStream_t st) {
   constexpr int LP = SmemShape<T, N, B, true>::LP;
   const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
   auto k = fft_real_kernel<T, C2R, N, B, AFF>;
   const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
   if (e != cudaSuccess) return e;
-  k<<<tiles, N / Vals<N>::value * B, smem, st>>>(A);
+  k<<<fast_grid(A), N / Vals<N>::value * B, smem, st>>>(with_table_offsets(A));
   return cudaGetLastError();
 }
 
 template <typename T, int N, bool C2R>
-static cudaError_t launch_real_n(const StageArgs& A, unsigned tiles, cudaStream_t st) {
+static cudaError_t launch_real_n(const StageArgs& A, cudaStream_t st) {
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
   if (A.src_line_affine || A.dst_line_affine)
-    return A.B == B0 ? launch_real_b<T, N, C2R, B0, true>(A, tiles, st) : cudaErrorInvalidValue;
-  if (A.B == B0) return launch_real_b<T, N, C2R, B0>(A, tiles, st);
-  if (A.B == B1) return launch_real_b<T, N, C2R, B1>(A, tiles, st);
-  if (A.B == B2) return launch_real_b<T, N, C2R, B2>(A, tiles, st);
+    return A.B == B0 ? launch_real_b<T, N, C2R, B0, true>(A, st) : cudaErrorInvalidValue;
+  if (A.B == B0) return launch_real_b<T, N, C2R, B0>(A, st);
+  if (A.B == B1) return launch_real_b<T, N, C2R, B1>(A, st);
+  if (A.B == B2) return launch_real_b<T, N, C2R, B2>(A, st);
   return cudaErrorInvalidValue;
 }
 
@@ -644,12 +673,12 @@ bool fast_stage_supported(int n) {
          n == 24 || n == 48 || n == 96 || n == 192 || n == 384 || n == 768;
 }
 
-cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, unsigned tiles,
-                            cudaStream_t st) {
+cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, cudaStream_t st) {
+  if (A.Eo0 > fast_stage_max_grid_yz() || A.Eo1 > fast_stage_max_grid_yz()) return cudaErrorInvalidValue;
 #define DFFT_CASE(N_)                                                                 \
   case N_:                                                                            \
-    return dbl ? launch_fast_t<double, N_>(A, inverse, afast, tiles, st)              \
-               : launch_fast_t<float, N_>(A, inverse, afast, tiles, st);
+    return dbl ? launch_fast_t<double, N_>(A, inverse, afast, st)                     \
+               : launch_fast_t<float, N_>(A, inverse, afast, st);
   switch (A.n) {
     DFFT_CASE(16)
     DFFT_CASE(32)
@@ -671,11 +700,12 @@ cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afa
 #undef DFFT_CASE
 }
 
-cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, unsigned tiles, cudaStream_t st) {
+cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, cudaStream_t st) {
+  if (A.Eo0 > fast_stage_max_grid_yz() || A.Eo1 > fast_stage_max_grid_yz()) return cudaErrorInvalidValue;
 #define DFFT_CASE(N_)                                                                          \
   case N_:                                                                                     \
-    if (dbl) return c2r ? launch_real_n<double, N_, true>(A, tiles, st) : launch_real_n<double, N_, false>(A, tiles, st); \
-    return c2r ? launch_real_n<float, N_, true>(A, tiles, st) : launch_real_n<float, N_, false>(A, tiles, st);
+    if (dbl) return c2r ? launch_real_n<double, N_, true>(A, st) : launch_real_n<double, N_, false>(A, st); \
+    return c2r ? launch_real_n<float, N_, true>(A, st) : launch_real_n<float, N_, false>(A, st);
   switch (A.n) {
     DFFT_CASE(16)
     DFFT_CASE(32)

@@ -224,8 +224,7 @@ dfft_status dfft_noalloc_impl(const void* in, void* out, int64_t n0, int64_t n1,
     A.scale = si == 2 ? scale : 1.0;
     A.tw = dbl ? static_cast<const void*>(s->tw64 + tw_offset(A.n))
                : static_cast<const void*>(s->tw32 + tw_offset(A.n));
-    const unsigned tiles = static_cast<unsigned>(A.tiles_b) * static_cast<unsigned>(A.Eo0);
-    if (launch_fft_fast(A, dbl, !fwd, a == 2, tiles, cs) != cudaSuccess) {
+    if (launch_fft_fast(A, dbl, !fwd, a == 2, cs) != cudaSuccess) {
       cudaGetLastError();
       *err = "FFT stage launch failed";
       return DFFT_ERROR_CUDA;

@@ -382,7 +382,10 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
     *affine = 1;
     return L.topo[a] == 1 && (!afast || layout_fast_axis(L) == a);
   };
-  const std::size_t Bf = dev::fast_stage_supported(static_cast<int>(n))
+  // the register kernels take the coordinates along o0 / o1 from a grid of
+  // (tiles, Eo0, Eo1) CTAs
+  const bool grid_ok = A.Eo0 <= dev::fast_stage_max_grid_yz() && A.Eo1 <= dev::fast_stage_max_grid_yz();
+  const std::size_t Bf = (grid_ok && dev::fast_stage_supported(static_cast<int>(n)))
                              ? static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)))
                              : 0;
   int saff = 0, daff = 0;
@@ -421,10 +424,9 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
 }
 
 // Launch of a register-resident stage (C2C, R2C or C2R).
-static cudaError_t launch_fast_op(const dev::StageArgs& A, bool dbl, int kind, bool inverse, unsigned tiles,
-                                  cudaStream_t st) {
-  if (kind == dev::kR2C || kind == dev::kC2R) return dev::launch_fft_fast_real(A, dbl, kind == dev::kC2R, tiles, st);
-  return dev::launch_fft_fast(A, dbl, inverse, A.load_afast != 0, tiles, st);
+static cudaError_t launch_fast_op(const dev::StageArgs& A, bool dbl, int kind, bool inverse, cudaStream_t st) {
+  if (kind == dev::kR2C || kind == dev::kC2R) return dev::launch_fft_fast_real(A, dbl, kind == dev::kC2R, st);
+  return dev::launch_fft_fast(A, dbl, inverse, A.load_afast != 0, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -905,12 +907,12 @@ void Plan::autotune() {
         dev::StageArgs T = A;
         T.in = s0;
         T.out = s1;
-        if (launch_fast_op(T, d_.dbl, op.kind, op.inverse, op.tiles, st) != cudaSuccess) {
+        if (launch_fast_op(T, d_.dbl, op.kind, op.inverse, st) != cudaSuccess) {
           cudaGetLastError();
           continue;
         }
         cudaEventRecord(e0, st);
-        for (int r = 0; r < 3; ++r) launch_fast_op(T, d_.dbl, op.kind, op.inverse, op.tiles, st);
+        for (int r = 0; r < 3; ++r) launch_fast_op(T, d_.dbl, op.kind, op.inverse, st);
         cudaEventRecord(e1, st);
         cuda_check(cudaEventSynchronize(e1), "tuner sync");
         float ms = 0.f;
@@ -949,7 +951,7 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
         A.in = buf(op0.src);
         A.out = buf(op0.dst);
         if (op0.fast)
-          e = launch_fast_op(A, d_.dbl, op0.kind, op0.inverse, op0.tiles, stream);
+          e = launch_fast_op(A, d_.dbl, op0.kind, op0.inverse, stream);
         else
           e = dev::launch_fft_stage(A, d_.dbl, op0.kind, op0.inverse, op0.nthreads, op0.smem, op0.tiles, stream);
         break;

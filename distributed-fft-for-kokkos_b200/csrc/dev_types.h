@@ -48,6 +48,10 @@ struct StageArgs {
   // b, o0, o1 in src.t / dst.t (filled by the launcher from src.off /
   // dst.off, so the kernels select no table at run time)
   int64_t s_ta, s_tb, s_to0, s_to1, d_ta, d_tb, d_to0, d_to1;
+  // register kernels: 1 = two complex64 lines per thread (fft_pair.cu), 2 =
+  // the same streaming tpc consecutive tiles along b per CTA
+  int pairs;
+  int tpc;
 };
 
 // Per-rank geometry of one transpose, packed as int64:
@@ -93,6 +97,15 @@ int fast_stage_line_options(bool dbl, int n, int* opts);
 cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, cudaStream_t st);
 cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, cudaStream_t st);
 constexpr int fast_stage_max_grid_yz() { return 65535; }
+// Two complex64 lines per thread (fft_pair.cu): C2C stages of 2^k points
+// (16..4096) on separable layouts; for b-fast tiles every line pair must start
+// on a 16-byte boundary (even offsets and stride along a).  A.B is the lines
+// per tile (twice the pairs), one of pair_stage_line_options().
+bool pair_stage_supported(int n);
+int pair_stage_line_options(int n, bool afast, int* opts);
+// Lines per tile of the streaming two-line variant (A.pairs = 2).
+int pair_stage_stream_lines(int n, bool afast);
+cudaError_t launch_fft_pair(const StageArgs& A, bool inverse, bool afast, cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
 cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);

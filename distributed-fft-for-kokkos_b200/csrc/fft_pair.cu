@@ -1,0 +1,406 @@
+// Register-resident FFT stage with two complex64 lines per thread (sm_100a).
+//
+// The same radix passes as fft_fast.cu (8 values a line per thread, lines of
+// 2^k points, 16..4096), but every thread carries two lines of the tile:
+//   b-fast tiles (unit stride along the tile axis b): lines 2l and 2l+1, which
+//     are neighbours in memory, so one 16-byte access moves the same position
+//     of both (the host checks that every pair starts on a 16-byte boundary);
+//   a-fast tiles (unit stride along the FFT axis a): lines l and l + B/2, each
+//     read as a contiguous row by consecutive threads.
+// The exchanges between passes move both lines' values of a position as one
+// 16-byte shared-memory element (the complex128 layout of the single-line
+// kernel, which keeps them conflict-free), and the twiddle reads, index and
+// address arithmetic of a thread serve 16 values instead of 8.  Separable
+// layouts only (per-axis offset tables, affine along a).
+#include "fft_radix.cuh"
+
+namespace dfft {
+namespace dev {
+
+using namespace radix;
+
+namespace {
+
+// One exchange of pass P for both lines of a pair: position p of the pair
+// lives at padpos(p) of the pair's shared-memory line as (x0, y0, x1, y1).
+template <int N, int P, int TT, int S>
+__device__ __forceinline__ void exchange_pair(float2* v0, float2* v1, int t, float4* line) {
+  constexpr int V = 8;
+  constexpr int R = Radix<N, P>::value, Q = V / R;
+  constexpr int R2 = Radix<N, P + 1>::value, Q2 = V / R2;
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float2 a = v0[q * R + r], b = v1[q * R + r];
+      line[padpos<S>(out_pos<N, P, TT>(t, q, r))] = make_float4(a.x, a.y, b.x, b.y);
+    }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q2; ++q)
+#pragma unroll
+    for (int r = 0; r < R2; ++r) {
+      const float4 w = line[padpos<S>(in_pos<N, P + 1, TT>(t, q, r))];
+      v0[q * R2 + r] = make_float2(w.x, w.y);
+      v1[q * R2 + r] = make_float2(w.z, w.w);
+    }
+  __syncthreads();
+}
+
+template <bool INV, int N, int P, int TT, int S>
+__device__ __forceinline__ void run_fft_pair(float2* v0, float2* v1, int t, const float2* tw, float4* line) {
+  // both lines read the same twiddles (same t): the second pass reuses them
+  compute_pass<float, INV, N, P, TT>(v0, t, tw);
+  compute_pass<float, INV, N, P, TT>(v1, t, tw);
+  if constexpr (P + 1 < Radix<N, 0>::npass) {
+    exchange_pair<N, P, TT, S>(v0, v1, t, line);
+    run_fft_pair<INV, N, P + 1, TT, S>(v0, v1, t, tw, line);
+  }
+}
+
+// Loads the pair (l0, l1) of one tile (first line b0) into v0 / v1.
+// b-fast: positions p of the pair at (line l0 offset) + p * stride; stride and
+// offsets are even (host check) and (N - 1) * stride < 2^31.
+template <int N, bool AFAST>
+__device__ __forceinline__ void load_pair(const StageArgs& A, const float2* in, int64_t so, int b0, int l0, int l1,
+                                          bool act0, bool act1, int t, float2* v0, float2* v1) {
+  using C = float2;
+  constexpr int V = 8, TT = N / V;
+  constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
+  const DevLayout& ls = A.src;
+  const C zero = make_float2(0.f, 0.f);
+  if (AFAST) {
+    const C* row0 = in + so + (act0 ? __ldg(ls.t + A.s_tb + b0 + l0) : 0);
+    const C* row1 = in + so + (act1 ? __ldg(ls.t + A.s_tb + b0 + l1) : 0);
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int p = in_pos<N, 0, TT>(t, q, r);
+        v0[q * R0 + r] = act0 ? row0[p] : zero;
+        v1[q * R0 + r] = act1 ? row1[p] : zero;
+      }
+  } else {
+    const int st = static_cast<int>(A.src_astride);
+    const int64_t base = so + (act0 ? __ldg(ls.t + A.s_tb + b0 + l0) : 0) + static_cast<int64_t>(t) * st;
+    if (act1) {
+      const float4* row = reinterpret_cast<const float4*>(in + base);
+      const int st2 = st / 2;
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+          const float4 w = row[(TT * q + r * (N / R0)) * st2];
+          v0[q * R0 + r] = make_float2(w.x, w.y);
+          v1[q * R0 + r] = make_float2(w.z, w.w);
+        }
+    } else {
+      const C* row = in + base;
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+          v0[q * R0 + r] = act0 ? row[(TT * q + r * (N / R0)) * st] : zero;
+          v1[q * R0 + r] = zero;
+        }
+    }
+  }
+}
+
+// Scales (when the stage scales) and stores the pair after the last pass.
+template <int N, bool AFAST>
+__device__ __forceinline__ void store_pair(const StageArgs& A, float2* out, int64_t dof, int b0, int l0, int l1,
+                                           bool act0, bool act1, int t, float2* v0, float2* v1) {
+  using C = float2;
+  constexpr int V = 8, TT = N / V;
+  constexpr int NPASS = Radix<N, 0>::npass;
+  constexpr int RL = Radix<N, NPASS - 1>::value, QL = V / RL;
+  const DevLayout& ld = A.dst;
+  if (A.scale != 1.0) {
+    const float s = static_cast<float>(A.scale);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      v0[e] = cscale(v0[e], s);
+      v1[e] = cscale(v1[e], s);
+    }
+  }
+  if (AFAST) {
+    C* row0 = out + dof + (act0 ? __ldg(ld.t + A.d_tb + b0 + l0) : 0);
+    C* row1 = out + dof + (act1 ? __ldg(ld.t + A.d_tb + b0 + l1) : 0);
+#pragma unroll
+    for (int q = 0; q < QL; ++q)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int p = t + last_rel<N, TT>(q, r);
+        if (act0) row0[p] = v0[q * RL + r];
+        if (act1) row1[p] = v1[q * RL + r];
+      }
+  } else if (act0) {
+    const int st = static_cast<int>(A.dst_astride);
+    const int64_t base = dof + __ldg(ld.t + A.d_tb + b0 + l0) + static_cast<int64_t>(t) * st;
+    if (act1) {
+      float4* row = reinterpret_cast<float4*>(out + base);
+      const int st2 = st / 2;
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const C a = v0[q * RL + r], b = v1[q * RL + r];
+          row[last_rel<N, TT>(q, r) * st2] = make_float4(a.x, a.y, b.x, b.y);
+        }
+    } else {
+      C* row = out + base;
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) row[last_rel<N, TT>(q, r) * st] = v0[q * RL + r];
+    }
+  }
+}
+
+// 1024 resident threads per SM: 64 registers for 16 complex64 values a thread
+template <int THREADS>
+struct PairMinBlocks {
+  static constexpr int v = 1024 / THREADS;
+  static constexpr int value = v > 0 ? v : 1;
+};
+
+// PB line pairs per CTA (2 PB lines), N/8 threads per pair.
+template <bool INV, int N, int PB, bool AFAST>
+__global__ void __launch_bounds__(N / 8 * PB, (PairMinBlocks<N / 8 * PB>::value)) fft_pair_kernel(const StageArgs A) {
+  using C = float2;
+  constexpr int V = 8;
+  static_assert(Vals<N>::value == V, "two-line kernel: lines of 2^k points");
+  constexpr int TT = N / V;
+  using SH = SmemShape<double, N, PB, AFAST>;  // 16-byte elements: the complex128 line layout
+  constexpr int LP = SH::LP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  float4* tile = reinterpret_cast<float4*>(smem_raw + sizeof(C) * N);
+  const DevLayout ls = A.src, ld = A.dst;
+
+  // grid (tiles_b, Eo0, Eo1)
+  const int b0 = blockIdx.x * 2 * PB, co0 = blockIdx.y, co1 = blockIdx.z;
+  const int nb = min(2 * PB, A.Eb - b0);
+  int lp, t;
+  if (AFAST) {
+    t = threadIdx.x % TT;
+    lp = threadIdx.x / TT;
+  } else {
+    lp = threadIdx.x % PB;
+    t = threadIdx.x / PB;
+  }
+  const int l0 = AFAST ? lp : 2 * lp, l1 = AFAST ? lp + PB : 2 * lp + 1;
+  const bool act0 = l0 < nb, act1 = l1 < nb;
+
+  {
+    const C* gtw = reinterpret_cast<const C*>(A.tw);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  }
+  int64_t so = A.src_abase, dof = A.dst_abase;
+  if (A.o0 >= 0) {
+    so += __ldg(ls.t + A.s_to0 + co0);
+    dof += __ldg(ld.t + A.d_to0 + co0);
+  }
+  if (A.o1 >= 0) {
+    so += __ldg(ls.t + A.s_to1 + co1);
+    dof += __ldg(ld.t + A.d_to1 + co1);
+  }
+
+  C v0[V], v1[V];
+  const C* in = reinterpret_cast<const C*>(A.in);
+  load_pair<N, AFAST>(A, in, so, b0, l0, l1, act0, act1, t, v0, v1);
+  __syncthreads();  // twiddles staged
+
+  run_fft_pair<INV, N, 0, TT, SH::S>(v0, v1, t, tw, tile + lp * LP);
+
+  store_pair<N, AFAST>(A, reinterpret_cast<C*>(A.out), dof, b0, l0, l1, act0, act1, t, v0, v1);
+}
+
+// Streaming variant: a CTA walks A.tpc consecutive tiles along b (grid
+// (ceil(tiles_b / tpc), Eo0, Eo1)) and issues the loads of tile i + 1 into
+// registers before it transforms tile i, so each thread keeps one tile's
+// loads in flight while it computes.  The table offsets along o0 / o1 and the
+// twiddles are set up once per CTA.  About 100 registers: one CTA per SM.
+template <bool INV, int N, int PB, bool AFAST>
+__global__ void __launch_bounds__(N / 8 * PB, 1) fft_pair_stream_kernel(const StageArgs A) {
+  using C = float2;
+  constexpr int V = 8;
+  static_assert(Vals<N>::value == V, "two-line kernel: lines of 2^k points");
+  constexpr int TT = N / V;
+  using SH = SmemShape<double, N, PB, AFAST>;
+  constexpr int LP = SH::LP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  float4* tile = reinterpret_cast<float4*>(smem_raw + sizeof(C) * N);
+  const DevLayout ls = A.src, ld = A.dst;
+
+  const int first = blockIdx.x * A.tpc, co0 = blockIdx.y, co1 = blockIdx.z;
+  const int last = min(first + A.tpc, A.tiles_b);
+  int lp, t;
+  if (AFAST) {
+    t = threadIdx.x % TT;
+    lp = threadIdx.x / TT;
+  } else {
+    lp = threadIdx.x % PB;
+    t = threadIdx.x / PB;
+  }
+  const int l0 = AFAST ? lp : 2 * lp, l1 = AFAST ? lp + PB : 2 * lp + 1;
+  {
+    const C* gtw = reinterpret_cast<const C*>(A.tw);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  }
+  int64_t so = A.src_abase, dof = A.dst_abase;
+  if (A.o0 >= 0) {
+    so += __ldg(ls.t + A.s_to0 + co0);
+    dof += __ldg(ld.t + A.d_to0 + co0);
+  }
+  if (A.o1 >= 0) {
+    so += __ldg(ls.t + A.s_to1 + co1);
+    dof += __ldg(ld.t + A.d_to1 + co1);
+  }
+  const C* in = reinterpret_cast<const C*>(A.in);
+  C* out = reinterpret_cast<C*>(A.out);
+
+  C v0[V], v1[V], w0[V], w1[V];
+  int b0 = first * 2 * PB;
+  int nb = min(2 * PB, A.Eb - b0);
+  load_pair<N, AFAST>(A, in, so, b0, l0, l1, l0 < nb, l1 < nb, t, v0, v1);
+  __syncthreads();  // twiddles staged
+  for (int k = first; k < last; ++k) {
+    const int bn = b0 + 2 * PB;
+    const int nbn = min(2 * PB, A.Eb - bn);
+    if (k + 1 < last) load_pair<N, AFAST>(A, in, so, bn, l0, l1, l0 < nbn, l1 < nbn, t, w0, w1);
+    run_fft_pair<INV, N, 0, TT, SH::S>(v0, v1, t, tw, tile + lp * LP);  // ends on a barrier
+    store_pair<N, AFAST>(A, out, dof, b0, l0, l1, l0 < nb, l1 < nb, t, v0, v1);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      v0[e] = w0[e];
+      v1[e] = w1[e];
+    }
+    b0 = bn;
+    nb = nbn;
+  }
+}
+
+// Line pairs per CTA, option i (0 default, 1 half, 2 double or quarter):
+//   b-fast: 8 pairs (16-line, 128-byte rows) or enough for 256 threads;
+//   a-fast: enough pairs for 128 threads;  at most 1024 threads.
+constexpr int pair_option(int n, bool afast, int i) {
+  const int tt = n / 8;
+  const int cap = 1024 / tt > 0 ? 1024 / tt : 1;
+  int p0 = afast ? (128 / tt > 1 ? 128 / tt : 1) : (256 / tt > 8 ? 256 / tt : 8);
+  if (p0 > cap) p0 = cap;
+  if (i == 0) return p0;
+  if (i == 1) return p0 / 2 > 0 ? p0 / 2 : 0;
+  if (p0 * 2 <= cap) return p0 * 2;
+  return p0 / 4 > 0 ? p0 / 4 : 0;
+}
+
+template <int N, bool INV, bool AF, int PB>
+static cudaError_t launch_pair_b(const StageArgs& A, cudaStream_t st) {
+  if constexpr (PB <= 0) {
+    return cudaErrorInvalidValue;
+  } else {
+    constexpr int LP = SmemShape<double, N, PB, AF>::LP;
+    const size_t smem = sizeof(float2) * N + sizeof(float4) * static_cast<size_t>(PB) * LP;
+    auto k = fft_pair_kernel<INV, N, PB, AF>;
+    const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
+    if (e != cudaSuccess) return e;
+    k<<<fast_grid(A), N / 8 * PB, smem, st>>>(with_table_offsets(A));
+    return cudaGetLastError();
+  }
+}
+
+// Line pairs per CTA of the streaming variant: the default, at most 512
+// threads (about 110 registers a thread leave room for one 512-thread CTA).
+constexpr int stream_pairs(int n, bool afast) {
+  const int p0 = pair_option(n, afast, 0);
+  const int cap = 512 / (n / 8) > 0 ? 512 / (n / 8) : 1;
+  return p0 < cap ? p0 : cap;
+}
+
+template <int N, bool INV, bool AF>
+static cudaError_t launch_pair_stream(const StageArgs& A, cudaStream_t st) {
+  constexpr int PB = stream_pairs(N, AF);
+  if (A.B != 2 * PB || A.tpc < 1) return cudaErrorInvalidValue;
+  constexpr int LP = SmemShape<double, N, PB, AF>::LP;
+  const size_t smem = sizeof(float2) * N + sizeof(float4) * static_cast<size_t>(PB) * LP;
+  auto k = fft_pair_stream_kernel<INV, N, PB, AF>;
+  const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid(static_cast<unsigned>((A.tiles_b + A.tpc - 1) / A.tpc), static_cast<unsigned>(A.Eo0),
+                  static_cast<unsigned>(A.Eo1));
+  k<<<grid, N / 8 * PB, smem, st>>>(with_table_offsets(A));
+  return cudaGetLastError();
+}
+
+template <int N, bool INV, bool AF>
+static cudaError_t launch_pair_n(const StageArgs& A, cudaStream_t st) {
+  constexpr int P0 = pair_option(N, AF, 0), P1 = pair_option(N, AF, 1), P2 = pair_option(N, AF, 2);
+  if (A.B == 2 * P0) return launch_pair_b<N, INV, AF, P0>(A, st);
+  if (P1 > 0 && A.B == 2 * P1) return launch_pair_b<N, INV, AF, P1>(A, st);
+  if (P2 > 0 && A.B == 2 * P2) return launch_pair_b<N, INV, AF, P2>(A, st);
+  return cudaErrorInvalidValue;
+}
+
+template <int N>
+static cudaError_t launch_pair_t(const StageArgs& A, bool inverse, bool afast, cudaStream_t st) {
+  if (A.pairs == 2) {
+    if (inverse) return afast ? launch_pair_stream<N, true, true>(A, st) : launch_pair_stream<N, true, false>(A, st);
+    return afast ? launch_pair_stream<N, false, true>(A, st) : launch_pair_stream<N, false, false>(A, st);
+  }
+  if (inverse) return afast ? launch_pair_n<N, true, true>(A, st) : launch_pair_n<N, true, false>(A, st);
+  return afast ? launch_pair_n<N, false, true>(A, st) : launch_pair_n<N, false, false>(A, st);
+}
+
+}  // namespace
+
+bool pair_stage_supported(int n) { return n >= 16 && n <= 4096 && (n & (n - 1)) == 0; }
+
+int pair_stage_stream_lines(int n, bool afast) {
+  switch (n) {
+#define DFFT_OPT(N_) \
+  case N_: return 2 * stream_pairs(N_, afast);
+    DFFT_OPT(16) DFFT_OPT(32) DFFT_OPT(64) DFFT_OPT(128) DFFT_OPT(256) DFFT_OPT(512) DFFT_OPT(1024) DFFT_OPT(2048)
+    DFFT_OPT(4096)
+#undef DFFT_OPT
+    default: return 0;
+  }
+}
+
+int pair_stage_line_options(int n, bool afast, int* opts) {
+  int k = 0;
+  for (int i = 0; i < 3; ++i) {
+    int p = 0;
+    switch (n) {
+#define DFFT_OPT(N_) \
+  case N_: p = pair_option(N_, afast, i); break;
+      DFFT_OPT(16) DFFT_OPT(32) DFFT_OPT(64) DFFT_OPT(128) DFFT_OPT(256) DFFT_OPT(512) DFFT_OPT(1024) DFFT_OPT(2048)
+      DFFT_OPT(4096)
+#undef DFFT_OPT
+      default: break;
+    }
+    if (p > 0) opts[k++] = 2 * p;
+  }
+  return k;
+}
+
+cudaError_t launch_fft_pair(const StageArgs& A, bool inverse, bool afast, cudaStream_t st) {
+  if (A.Eo0 > fast_stage_max_grid_yz() || A.Eo1 > fast_stage_max_grid_yz()) return cudaErrorInvalidValue;
+  switch (A.n) {
+    case 16: return launch_pair_t<16>(A, inverse, afast, st);
+    case 32: return launch_pair_t<32>(A, inverse, afast, st);
+    case 64: return launch_pair_t<64>(A, inverse, afast, st);
+    case 128: return launch_pair_t<128>(A, inverse, afast, st);
+    case 256: return launch_pair_t<256>(A, inverse, afast, st);
+    case 512: return launch_pair_t<512>(A, inverse, afast, st);
+    case 1024: return launch_pair_t<1024>(A, inverse, afast, st);
+    case 2048: return launch_pair_t<2048>(A, inverse, afast, st);
+    case 4096: return launch_pair_t<4096>(A, inverse, afast, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace dev
+}  // namespace dfft

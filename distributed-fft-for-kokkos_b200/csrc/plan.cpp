@@ -416,6 +416,33 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
     A.src_astride = sas;
     A.dst_abase = dab;
     A.dst_astride = das;
+    // Two complex64 lines per thread: C2C of 2^k points on separable sides;
+    // b-fast tiles move both lines of a pair with one 16-byte access, so
+    // every pair must start on an even element on both sides.
+    auto pair_aligned = [&](int l, std::int64_t abase, std::int64_t astride) {
+      const LayoutTables& T = tables_[l];
+      if (T.mode != 0 || (abase & 1) || (astride & 1)) return false;
+      const std::int64_t* ob = T.data.data() + T.off[b];
+      for (std::size_t c = 0; c + 1 < static_cast<std::size_t>(A.Eb); c += 2)
+        if ((ob[c] & 1) || ob[c + 1] != ob[c] + 1) return false;
+      if ((A.Eb & 1) && (ob[A.Eb - 1] & 1)) return false;
+      for (int o : {A.o0, A.o1}) {
+        if (o < 0) continue;
+        const std::int64_t* oo = T.data.data() + T.off[o];
+        for (std::size_t c = 0; c < layouts_[l].gext[o]; ++c)
+          if (oo[c] & 1) return false;
+      }
+      return true;
+    };
+    if (kind == dev::kC2C && !d_.dbl && dev::pair_stage_supported(static_cast<int>(n)) && !saff && !daff &&
+        (A.load_afast || (pair_aligned(src_l, sab, sas) && pair_aligned(dst_l, dab, das)))) {
+      int opts[3];
+      dev::pair_stage_line_options(static_cast<int>(n), A.load_afast != 0, opts);
+      op.single_B = A.B;
+      A.pairs = 1;
+      A.B = opts[0];
+      A.tiles_b = static_cast<int>((Dl.gext[b] + opts[0] - 1) / opts[0]);
+    }
     const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
     if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
     op.tiles = static_cast<unsigned>(ft);
@@ -426,6 +453,7 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
 // Launch of a register-resident stage (C2C, R2C or C2R).
 static cudaError_t launch_fast_op(const dev::StageArgs& A, bool dbl, int kind, bool inverse, cudaStream_t st) {
   if (kind == dev::kR2C || kind == dev::kC2R) return dev::launch_fft_fast_real(A, dbl, kind == dev::kC2R, st);
+  if (A.pairs) return dev::launch_fft_pair(A, inverse, A.load_afast != 0, st);
   return dev::launch_fft_fast(A, dbl, inverse, A.load_afast != 0, st);
 }
 
@@ -828,7 +856,8 @@ void Plan::allocate_device() {
 }
 
 // ---------------------------------------------------------------------------
-// Autotuner: lines per CTA of every register-resident stage, timed on the
+// Autotuner: kernel variant (one or two lines per thread) and lines per CTA
+// of every register-resident stage, timed on the
 // plan's scratch buffers at plan creation and cached per stage signature
 // (line length, precision, direction, row orientation, tile grid) for the
 // process; DFFT_TUNE_CACHE=<file> also persists the choices across processes
@@ -875,18 +904,30 @@ void Plan::autotune() {
       dev::StageArgs& A = op.sa;
       if (A.src_line_affine || A.dst_line_affine) continue;  // general layouts keep the default tile
       std::ostringstream k;
-      const bool pairs = op.kind == dev::kR2C || op.kind == dev::kC2R;
+      const bool real = op.kind == dev::kR2C || op.kind == dev::kC2R;  // two real lines per register line
+      const bool pair_ok = op.single_B != 0;                            // eligible for two lines per thread
       k << "fast:n" << A.n << (d_.dbl ? "f64" : "f32") << (op.inverse ? "i" : "f") << (A.load_afast ? "a" : "b")
-        << (op.kind == dev::kR2C ? "r2c" : op.kind == dev::kC2R ? "c2r" : "") << ":" << A.Eb << "x" << A.Eo0 << "x"
-        << A.Eo1;
+        << (op.kind == dev::kR2C ? "r2c" : op.kind == dev::kC2R ? "c2r" : "") << (pair_ok ? "P" : "") << ":" << A.Eb
+        << "x" << A.Eo0 << "x" << A.Eo1;
       const std::string key = k.str();
-      auto apply = [&](int B) {
-        A.B = B;
-        A.tiles_b = pairs ? (A.Eb + 2 * B - 1) / (2 * B) : (A.Eb + B - 1) / B;
+      // a configuration: lines per tile of the one-line kernel; kPairCode +
+      // lines per tile of the two-line kernel; kStreamCode + tiles per CTA of
+      // its streaming variant
+      constexpr int kPairCode = 100000, kStreamCode = 200000;
+      auto apply = [&](int code) {
+        if (code >= kStreamCode) {
+          A.pairs = 2;
+          A.tpc = code - kStreamCode;
+          A.B = dev::pair_stage_stream_lines(A.n, A.load_afast != 0);
+        } else {
+          A.pairs = code >= kPairCode ? 1 : 0;
+          A.B = code % kPairCode;
+        }
+        A.tiles_b = real ? (A.Eb + 2 * A.B - 1) / (2 * A.B) : (A.Eb + A.B - 1) / A.B;
         op.tiles = static_cast<unsigned>(static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1);
       };
       auto it = g_tune_cache.find(key);
-      if (it != g_tune_cache.end()) {
+      if (it != g_tune_cache.end() && (it->second < kPairCode || pair_ok)) {
         apply(it->second);
         continue;
       }
@@ -895,15 +936,25 @@ void Plan::autotune() {
         cuda_check(cudaMemsetAsync(s1, 0, buf_bytes_[kBufScratch1], st), "tuner clear");
         cleared = true;
       }
+      std::vector<int> cand;
       int opts[4];
+      if (pair_ok) {
+        const int np = dev::pair_stage_line_options(A.n, A.load_afast != 0, opts);
+        for (int i = 0; i < np; ++i) cand.push_back(kPairCode + opts[i]);
+        const int sb = dev::pair_stage_stream_lines(A.n, A.load_afast != 0);
+        const int tiles = sb > 0 ? (A.Eb + sb - 1) / sb : 0;
+        for (int tpc : {4, 8, 16})
+          if (tiles >= 2 * tpc) cand.push_back(kStreamCode + tpc);
+      }
       const int nopt = dev::fast_stage_line_options(d_.dbl, A.n, opts);
-      int best = A.B;
+      for (int i = 0; i < nopt; ++i) cand.push_back(opts[i]);
+      int best = A.pairs == 2 ? kStreamCode + A.tpc : (A.pairs ? kPairCode : 0) + A.B;
       float best_ms = std::numeric_limits<float>::max();
       cudaEvent_t e0, e1;
       cuda_check(cudaEventCreate(&e0), "tuner event");
       cuda_check(cudaEventCreate(&e1), "tuner event");
-      for (int i = 0; i < nopt; ++i) {
-        apply(opts[i]);
+      for (int code : cand) {
+        apply(code);
         dev::StageArgs T = A;
         T.in = s0;
         T.out = s1;
@@ -919,7 +970,7 @@ void Plan::autotune() {
         cudaEventElapsedTime(&ms, e0, e1);
         if (ms < best_ms) {
           best_ms = ms;
-          best = opts[i];
+          best = code;
         }
       }
       cudaEventDestroy(e0);
@@ -950,6 +1001,13 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
         dev::StageArgs A = op0.sa;
         A.in = buf(op0.src);
         A.out = buf(op0.dst);
+        if (op0.fast && A.pairs && !A.load_afast &&
+            ((reinterpret_cast<std::uintptr_t>(A.in) | reinterpret_cast<std::uintptr_t>(A.out)) & 15)) {
+          // a caller buffer off a 16-byte boundary: the one-line kernel
+          A.pairs = 0;
+          A.B = op0.single_B;
+          A.tiles_b = (A.Eb + A.B - 1) / A.B;
+        }
         if (op0.fast)
           e = launch_fast_op(A, d_.dbl, op0.kind, op0.inverse, stream);
         else

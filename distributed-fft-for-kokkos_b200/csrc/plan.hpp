@@ -37,7 +37,9 @@ struct Op {
   dev::StageArgs sa{};
   int kind = 0;
   bool inverse = false;
-  bool fast = false;  // register-resident power-of-two kernel
+  bool fast = false;  // register-resident kernel (fft_fast.cu, or fft_pair.cu when sa.pairs)
+  int single_B = 0;   // lines per tile of the one-line kernel, for b-fast pair stages whose
+                      // caller buffers turn out not to be 16-byte aligned
   int nthreads = 256;
   std::size_t smem = 0;
   unsigned tiles = 0;

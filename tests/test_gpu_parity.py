@@ -272,3 +272,31 @@ def test_register_kernels_on_ragged_blocks(gin, axes, tin, tout, real, precision
     # rank blocks of unequal size make the layout tables general (per-rank
     # strides); the register kernels then address each line as base + p * stride
     check_roundtrip(gin, axes, tin, tout, real, precision=precision)
+
+
+def test_fp32_pair_kernel_misaligned_buffers_fall_back():
+    """Two-lines-per-thread stages move line pairs with 16-byte accesses; a
+    caller buffer that is only complex64-aligned (8 bytes) runs the one-line
+    kernel instead, with bit-identical results."""
+    import torch
+    gin = (64, 64, 64)
+    plan = dfft.Plan(gin, gin, (0, 1, 2), (2, 2, 1), (1, 2, 2), precision="float32")
+    x = random_input(gin, False, 4, "float32")
+    flat = dfft.scatter_blocks(plan, x, "in")
+    n = flat.size
+    t_in = torch.from_numpy(np.ascontiguousarray(flat)).cuda()
+    store = torch.zeros(n + 1, dtype=torch.complex64, device="cuda")
+    aligned = store[:n]
+    shifted = store[1:]  # 8 bytes past a 16-byte boundary
+    ref = torch.empty(n, dtype=torch.complex64, device="cuda")
+    dfft.execute(plan, t_in, ref, dfft.Direction.forward)
+    dfft.execute(plan, t_in, shifted, dfft.Direction.forward)
+    torch.cuda.synchronize()
+    assert torch.equal(shifted.view(torch.float32), ref.view(torch.float32))
+    X = dfft.gather_blocks(plan, ref.cpu().numpy(), "out")
+    assert O.rel_l2(X, O.global_fft(x, (0, 1, 2), False)) <= TOL["float32"]
+    back_store = torch.zeros(n + 1, dtype=torch.complex64, device="cuda")
+    dfft.execute(plan, shifted.clone(), back_store[1:], dfft.Direction.backward)
+    dfft.execute(plan, ref, aligned, dfft.Direction.backward)
+    torch.cuda.synchronize()
+    assert torch.equal(back_store[1:].view(torch.float32), aligned.view(torch.float32))

@@ -505,6 +505,48 @@ dfft_status dfft_ns_energy(dfft_ns* ns, const void* uk, double* energy, void* st
   });
 }
 
+dfft_status dfft_ns_velocity(dfft_ns* ns, const void* uk, void* u, void* stream) {
+  return guarded([&] {
+    if (!uk || !u) dfft::fail(dfft::kErrInvalidArgument, "null buffer");
+    dfft::ns_velocity(ns_of(ns), uk, u, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_ns_vorticity(dfft_ns* ns, const void* uk, void* vor, void* stream) {
+  return guarded([&] {
+    if (!uk || !vor) dfft::fail(dfft::kErrInvalidArgument, "null buffer");
+    dfft::ns_vorticity(ns_of(ns), uk, vor, static_cast<cudaStream_t>(stream));
+  });
+}
+
+static_assert(DFFT_NS_MAX_BINS == dfft::kNsMaxBins, "spectrum bin limit");
+
+dfft_status dfft_ns_diagnostics(dfft_ns* ns, const void* uk, int32_t num_bins, double* e_spec, double* k_vals,
+                                dfft_ns_diag* out, void* stream) {
+  return guarded([&] {
+    if (!uk || !out) dfft::fail(dfft::kErrInvalidArgument, "null argument");
+    const dfft::NsDiag d = dfft::ns_diagnostics(ns_of(ns), uk, num_bins, e_spec, k_vals,
+                                                static_cast<cudaStream_t>(stream));
+    out->energy = d.energy;
+    out->enstrophy = d.enstrophy;
+    out->divergence_l2 = d.divergence_l2;
+  });
+}
+
+dfft_status dfft_ns_write_diagnostics(dfft_ns* ns, const void* uk, const char* out_dir, int32_t iter,
+                                      int32_t num_bins, dfft_ns_diag* out, void* stream) {
+  return guarded([&] {
+    if (!uk || !out_dir) dfft::fail(dfft::kErrInvalidArgument, "null argument");
+    const dfft::NsDiag d = dfft::ns_write_diagnostics(ns_of(ns), uk, out_dir, iter, num_bins,
+                                                      static_cast<cudaStream_t>(stream));
+    if (out) {
+      out->energy = d.energy;
+      out->enstrophy = d.enstrophy;
+      out->divergence_l2 = d.divergence_l2;
+    }
+  });
+}
+
 dfft_status dfft_ns_destroy(dfft_ns* ns) {
   return guarded([&] {
     if (!ns) return;

@@ -13,12 +13,15 @@
 // global wavenumber of each element whatever the topology.  The RK4 stage
 // update is fused into the combine / projection kernel.
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <vector>
 #include <new>
 #include <string>
 
 #include "../../include/dfft.h"
 #include "fft_stage.cuh"
+#include "layout.hpp"
 #include "ns.hpp"
 #include "plan.hpp"
 
@@ -227,6 +230,100 @@ __global__ void ns_energy_kernel(const DevLayout L, const cplx<T>* uk, NsGeom g,
   if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
 }
 
+// vorticity spectrum i k x u_hat with the full (not dealiased) wavenumbers
+// (compute_vorticity, main.cpp:677-698)
+template <typename T>
+__global__ void ns_vorticity_kernel(const DevLayout L, const cplx<T>* uk, cplx<T>* w, NsGeom g) {
+  const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int iz = static_cast<int>(t % g.nzh);
+    const int iy = static_cast<int>((t / g.nzh) % g.ny);
+    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    const T kx = T(signed_mode(ix, g.nx) * g.kscale), ky = T(signed_mode(iy, g.ny) * g.kscale),
+            kz = T(iz * g.kscale);
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
+    const cplx<T> u = uk[o[0]], v = uk[o[1]], q = uk[o[2]];
+    // c = k x u_hat, then i c = (-c.y, c.x)
+    const cplx<T> c0 = mk<T>(ky * q.x - kz * v.x, ky * q.y - kz * v.y);
+    const cplx<T> c1 = mk<T>(kz * u.x - kx * q.x, kz * u.y - kx * q.y);
+    const cplx<T> c2 = mk<T>(kx * v.x - ky * u.x, kx * v.y - ky * u.y);
+    w[o[0]] = mk<T>(-c0.y, c0.x);
+    w[o[1]] = mk<T>(-c1.y, c1.x);
+    w[o[2]] = mk<T>(-c2.y, c2.x);
+  }
+}
+
+// FP64 diagnostics of a spectrum (diag_energy, main.cpp:741-794, plus the
+// enstrophy and the divergence): out[0] += coef * sum 0.5 f |u_hat|^2,
+// out[1] += coef * sum 0.5 f |k x u_hat|^2, out[2] += coef * sum f |k . u_hat|^2,
+// out[3 + i] += sum 0.5 f |u_hat|^2 over the modes with bins[i] <= |k| <
+// bins[i + 1] (no coef, as the reference's E_spec), f = 1 on the kz = 0 plane
+// and 2 elsewhere.  |k| is formed without fused multiply-adds so that it
+// rounds as k_x^2 + k_y^2 + k_z^2 evaluated term by term.
+template <typename T>
+__global__ void ns_diag_kernel(const DevLayout L, const cplx<T>* uk, NsGeom g, double coef, const double* bins,
+                               int nb, double* out) {
+  extern __shared__ double sh[];  // bins (nb + 1), then the nb spectrum sums of this CTA
+  double* sb = sh;
+  double* ss = sh + nb + 1;
+  for (int i = threadIdx.x; i <= nb; i += blockDim.x) sb[i] = bins[i];
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) ss[i] = 0.0;
+  __syncthreads();
+  const double delta = nb > 0 ? sb[nb] / nb : 0.0;
+  const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
+  double ae = 0.0, aw = 0.0, ad = 0.0;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int iz = static_cast<int>(t % g.nzh);
+    const int iy = static_cast<int>((t / g.nzh) % g.ny);
+    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    const double kx = signed_mode(ix, g.nx) * g.kscale, ky = signed_mode(iy, g.ny) * g.kscale, kz = iz * g.kscale;
+    const double f = (iz == 0) ? 1.0 : 2.0;
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
+    double ur[3], ui[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const cplx<T> v = uk[o[d]];
+      ur[d] = double(v.x);
+      ui[d] = double(v.y);
+    }
+    const double e = 0.5 * f * (ur[0] * ur[0] + ui[0] * ui[0] + ur[1] * ur[1] + ui[1] * ui[1] + ur[2] * ur[2] +
+                                ui[2] * ui[2]);
+    ae += e * coef;
+    const double c0r = ky * ur[2] - kz * ur[1], c0i = ky * ui[2] - kz * ui[1];
+    const double c1r = kz * ur[0] - kx * ur[2], c1i = kz * ui[0] - kx * ui[2];
+    const double c2r = kx * ur[1] - ky * ur[0], c2i = kx * ui[1] - ky * ui[0];
+    aw += 0.5 * f * coef * (c0r * c0r + c0i * c0i + c1r * c1r + c1i * c1i + c2r * c2r + c2i * c2i);
+    const double dr = kx * ur[0] + ky * ur[1] + kz * ur[2], di = kx * ui[0] + ky * ui[1] + kz * ui[2];
+    ad += f * coef * (dr * dr + di * di);
+    if (nb > 0) {
+      const double ksq = __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
+      const double km = sqrt(ksq);
+      int i = delta > 0.0 ? static_cast<int>(km / delta) : 0;
+      i = max(0, min(i, nb - 1));
+      while (i > 0 && km < sb[i]) --i;
+      while (i < nb - 1 && km >= sb[i + 1]) ++i;
+      if (km >= sb[i] && km < sb[i + 1]) atomicAdd(ss + i, e);
+    }
+  }
+  for (int s = 16; s > 0; s >>= 1) {
+    ae += __shfl_down_sync(0xffffffffu, ae, s);
+    aw += __shfl_down_sync(0xffffffffu, aw, s);
+    ad += __shfl_down_sync(0xffffffffu, ad, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, ae);
+    atomicAdd(out + 1, aw);
+    atomicAdd(out + 2, ad);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    if (ss[i] != 0.0) atomicAdd(out + 3 + i, ss[i]);
+}
+
 unsigned grid_of(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
@@ -250,6 +347,8 @@ struct NsState {
   void* du[3] = {nullptr, nullptr, nullptr};  // physical derivatives
   void* rk[4] = {nullptr, nullptr, nullptr, nullptr};  // y0, k1, k2, k3
   double* energy = nullptr;
+  double* diag = nullptr;  // 3 + kNsMaxBins sums of ns_diagnostics
+  double* bins = nullptr;  // kNsMaxBins + 1 bin edges
   ~NsState() {
     for (auto p : dk) cudaFree(p);
     for (auto p : du) cudaFree(p);
@@ -257,6 +356,8 @@ struct NsState {
     cudaFree(adv);
     cudaFree(u);
     cudaFree(energy);
+    cudaFree(diag);
+    cudaFree(bins);
   }
 };
 
@@ -300,6 +401,8 @@ NsState* ns_create(const Plan* plan, double nu, double dt, double lx) {
     ck(cudaMalloc(&s->adv, s->nout * cb), "ns alloc");
     ck(cudaMalloc(&s->u, s->nin * rb), "ns alloc");
     ck(cudaMalloc(reinterpret_cast<void**>(&s->energy), sizeof(double)), "ns alloc");
+    ck(cudaMalloc(reinterpret_cast<void**>(&s->diag), (3 + kNsMaxBins) * sizeof(double)), "ns alloc");
+    ck(cudaMalloc(reinterpret_cast<void**>(&s->bins), (kNsMaxBins + 1) * sizeof(double)), "ns alloc");
   } catch (...) {
     delete s;
     throw;
@@ -391,6 +494,122 @@ double ns_energy(NsState* s, const void* uk, cudaStream_t st) {
   ck(cudaMemcpyAsync(&e, s->energy, sizeof(double), cudaMemcpyDeviceToHost, st), "ns energy");
   ck(cudaStreamSynchronize(st), "ns energy");
   return e;
+}
+
+void ns_velocity(NsState* s, const void* uk, void* u, cudaStream_t st) { s->plan->execute(uk, u, false, st); }
+
+void ns_vorticity(NsState* s, const void* uk, void* vor, cudaStream_t st) {
+  using namespace dev;
+  const int64_t nsp = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nzh;
+  if (s->dbl)
+    ns_vorticity_kernel<double><<<grid_of(nsp), 256, 0, st>>>(s->lout, static_cast<const double2*>(uk),
+                                                               static_cast<double2*>(s->adv), s->g);
+  else
+    ns_vorticity_kernel<float><<<grid_of(nsp), 256, 0, st>>>(s->lout, static_cast<const float2*>(uk),
+                                                              static_cast<float2*>(s->adv), s->g);
+  ck(cudaGetLastError(), "ns vorticity");
+  s->plan->execute(s->adv, vor, false, st);
+}
+
+// Radial bins of the energy spectrum (main.cpp:471-500): k_max is the largest
+// |k| of the grid, the edges linspace(0, k_max, nb + 1) with the last edge
+// k_max itself, the k values the bin midpoints.
+static std::vector<double> spectrum_bins(const NsState* s, int nb) {
+  const double kx = (s->g.nx / 2) * s->g.kscale, ky = (s->g.ny / 2) * s->g.kscale, kz = (s->g.nz / 2) * s->g.kscale;
+  volatile double sq = kx * kx;  // evaluated term by term, as on the device
+  sq = sq + ky * ky;
+  sq = sq + kz * kz;
+  const double k_max = std::sqrt(static_cast<double>(sq));
+  std::vector<double> b(static_cast<std::size_t>(nb) + 1);
+  const double delta = (k_max - 0.0) / static_cast<double>(nb);
+  for (int i = 0; i < nb; ++i) b[i] = 0.0 + delta * static_cast<double>(i);
+  b[nb] = k_max;
+  return b;
+}
+
+NsDiag ns_diagnostics(NsState* s, const void* uk, int nb, double* spec, double* kvals, cudaStream_t st) {
+  using namespace dev;
+  if (nb < 0 || nb > kNsMaxBins)
+    fail(kErrInvalidArgument, "num_bins must be in [0, " + std::to_string(kNsMaxBins) + "]");
+  if (nb > 0 && (!spec || !kvals)) fail(kErrInvalidArgument, "null spectrum output");
+  const int64_t nsp = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nzh;
+  const double N = static_cast<double>(s->g.nx) * s->g.ny * s->g.nz;
+  const double vol = s->lx * 3.14159265358979323846;
+  std::vector<double> bins = nb > 0 ? spectrum_bins(s, nb) : std::vector<double>(1, 0.0);
+  ck(cudaMemcpyAsync(s->bins, bins.data(), bins.size() * sizeof(double), cudaMemcpyHostToDevice, st), "ns diag");
+  ck(cudaMemsetAsync(s->diag, 0, (3 + static_cast<std::size_t>(nb)) * sizeof(double), st), "ns diag");
+  const std::size_t smem = (2 * static_cast<std::size_t>(nb) + 1) * sizeof(double);
+  const double coef = vol * vol * vol / (N * N);
+  if (s->dbl)
+    ns_diag_kernel<double><<<grid_of(nsp), 256, smem, st>>>(s->lout, static_cast<const double2*>(uk), s->g, coef,
+                                                             s->bins, nb, s->diag);
+  else
+    ns_diag_kernel<float><<<grid_of(nsp), 256, smem, st>>>(s->lout, static_cast<const float2*>(uk), s->g, coef,
+                                                            s->bins, nb, s->diag);
+  ck(cudaGetLastError(), "ns diag");
+  std::vector<double> h(3 + static_cast<std::size_t>(nb));
+  ck(cudaMemcpyAsync(h.data(), s->diag, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "ns diag");
+  ck(cudaStreamSynchronize(st), "ns diag");
+  for (int i = 0; i < nb; ++i) {
+    spec[i] = h[3 + i];
+    kvals[i] = 0.5 * (bins[i] + bins[i + 1]);
+  }
+  NsDiag d;
+  d.energy = h[0];
+  d.enstrophy = h[1];
+  d.divergence_l2 = std::sqrt(h[2]);
+  return d;
+}
+
+// "<dir>/<label>_rx<3 digits>_ry<3 digits>_<10 digits>.dat" (main.cpp:803-818,
+// IO::zfill)
+static std::string dump_name(const std::string& dir, const char* label, std::size_t rx, std::size_t ry, int iter) {
+  char tail[64];
+  std::snprintf(tail, sizeof(tail), "_rx%03zu_ry%03zu_%010d.dat", rx, ry, iter);
+  return dir + "/" + label + tail;
+}
+
+static void write_raw(const std::string& path, const void* data, std::size_t bytes) {
+  std::FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) fail(kErrInvalidArgument, "Failed to open file: " + path);
+  const std::size_t w = bytes ? std::fwrite(data, 1, bytes, f) : 0;
+  const int c = std::fclose(f);
+  if (w != bytes || c != 0) fail(kErrInternal, "short write to " + path);
+}
+
+NsDiag ns_write_diagnostics(NsState* s, const void* uk, const std::string& dir, int iter, int nb, cudaStream_t st) {
+  const auto& d = s->plan->desc();
+  if (d.in_topo[0] != 1 || d.in_topo[3] != 1)
+    fail(kErrUnsupported, "field dumps name files by (rx, ry) of the reference's in_topology (1, px, py, 1)");
+  if (iter < 0) fail(kErrInvalidArgument, "iteration must be non-negative");
+  const std::size_t rb = s->dbl ? 8 : 4;
+  std::vector<unsigned char> host(s->nin * rb);
+  const auto blocks = layout_blocks(s->plan->in_layout());
+  auto dump = [&](const char* const labels[3]) {
+    ck(cudaMemcpyAsync(host.data(), s->u, host.size(), cudaMemcpyDeviceToHost, st), "ns dump");
+    ck(cudaStreamSynchronize(st), "ns dump");
+    for (const RankBlock& b : blocks) {
+      // LayoutRight block (3, nx_loc, ny_loc, nz): component c is one contiguous run
+      const std::size_t comp = b.size / 3;
+      for (int c = 0; c < 3; ++c)
+        write_raw(dump_name(dir, labels[c], b.coords[1], b.coords[2], iter),
+                  host.data() + (b.base + c * comp) * rb, comp * rb);
+    }
+  };
+  // diag_fields (main.cpp:711-739): velocity, then vorticity, in physical space
+  ns_velocity(s, uk, s->u, st);
+  static const char* const vel[3] = {"u", "v", "w"};
+  dump(vel);
+  ns_vorticity(s, uk, s->u, st);
+  static const char* const vor[3] = {"vor_x", "vor_y", "vor_z"};
+  dump(vor);
+  // diag_energy (main.cpp:741-794): spectrum and bin centres, written once
+  // (by rank 0 in the reference, whose coordinates are (0, 0))
+  std::vector<double> spec(static_cast<std::size_t>(nb)), kv(static_cast<std::size_t>(nb));
+  NsDiag r = ns_diagnostics(s, uk, nb, spec.data(), kv.data(), st);
+  write_raw(dump_name(dir, "E_spec", 0, 0, iter), spec.data(), spec.size() * sizeof(double));
+  write_raw(dump_name(dir, "k_vals", 0, 0, iter), kv.data(), kv.size() * sizeof(double));
+  return r;
 }
 
 void ns_destroy(NsState* s) { delete s; }

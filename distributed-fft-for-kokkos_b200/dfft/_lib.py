@@ -70,6 +70,12 @@ class TransBlockDesc(ctypes.Structure):
     ]
 
 
+class NsDiag(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("enstrophy", ctypes.c_double), ("divergence_l2", ctypes.c_double)]
+
+
+NS_MAX_BINS = 2048
+
 _U64P = ctypes.POINTER(ctypes.c_uint64)
 _I32P = ctypes.POINTER(ctypes.c_int32)
 
@@ -127,6 +133,14 @@ SIGNATURES = {
     "dfft_ns_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "dfft_ns_energy": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "dfft_ns_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_ns_vorticity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_ns_diagnostics": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(NsDiag), ctypes.c_void_p]),
+    "dfft_ns_write_diagnostics": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
+                       ctypes.POINTER(NsDiag), ctypes.c_void_p]),
     "dfft_ns_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dfft_pack": (
         ctypes.c_int, [ctypes.c_int32, _U64P, _I32P, ctypes.c_int32, _U64P, ctypes.c_int32, ctypes.c_int32,

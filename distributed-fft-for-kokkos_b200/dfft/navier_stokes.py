@@ -8,7 +8,7 @@ out_topology (1, 1, px, py) (main.cpp:96-102).
 """
 import ctypes
 
-from ._lib import lib
+from ._lib import NS_MAX_BINS, NsDiag, lib
 from .plan import _check, _ptr
 
 
@@ -16,8 +16,12 @@ class NavierStokes:
     """``NavierStokes(plan, nu, dt, lx)``: nu = 1 / Re, dt the time step, the
     domain [0, lx pi)^3.  Methods mirror the example's NavierStokes / RK4th
     members: ``init_taylor_green`` (Variables constructor, main.cpp:322-363),
-    ``rhs`` (main.cpp:536-586), ``step`` (solve, main.cpp:518-528) and
-    ``energy`` (diag_energy, main.cpp:746-766)."""
+    ``rhs`` (main.cpp:536-586), ``step`` (solve, main.cpp:518-528),
+    ``energy`` (diag_energy, main.cpp:746-766), ``velocity`` / ``vorticity``
+    (diag_fields / compute_vorticity, main.cpp:677-724), ``diagnostics``
+    (FP64 energy, enstrophy, divergence and the energy spectrum of
+    diag_energy, main.cpp:741-794) and ``write_diagnostics`` (the example's
+    binary files, main.cpp:705-818)."""
 
     def __init__(self, plan, nu=0.01, dt=0.01, lx=2.0):
         self._plan = plan  # the plan must outlive the state
@@ -41,6 +45,31 @@ class NavierStokes:
         e = ctypes.c_double(0.0)
         _check(lib.dfft_ns_energy(self._h, _ptr(uk), ctypes.byref(e), self._stream(stream)))
         return e.value
+
+    def velocity(self, uk, u, stream=None):
+        _check(lib.dfft_ns_velocity(self._h, _ptr(uk), _ptr(u), self._stream(stream)))
+
+    def vorticity(self, uk, vor, stream=None):
+        _check(lib.dfft_ns_vorticity(self._h, _ptr(uk), _ptr(vor), self._stream(stream)))
+
+    def diagnostics(self, uk, num_bins=50, stream=None):
+        """dict(energy, enstrophy, divergence_l2, e_spec, k_vals); the sums are FP64."""
+        if not 0 <= num_bins <= NS_MAX_BINS:
+            raise ValueError(f"num_bins must be in [0, {NS_MAX_BINS}]")
+        spec = (ctypes.c_double * max(num_bins, 1))()
+        kv = (ctypes.c_double * max(num_bins, 1))()
+        d = NsDiag()
+        _check(lib.dfft_ns_diagnostics(self._h, _ptr(uk), int(num_bins), spec, kv, ctypes.byref(d),
+                                       self._stream(stream)))
+        return {"energy": d.energy, "enstrophy": d.enstrophy, "divergence_l2": d.divergence_l2,
+                "e_spec": list(spec)[:num_bins], "k_vals": list(kv)[:num_bins]}
+
+    def write_diagnostics(self, uk, out_dir, iteration, num_bins=50, stream=None):
+        """The example's per-rank velocity / vorticity files and the spectrum files of one iteration."""
+        d = NsDiag()
+        _check(lib.dfft_ns_write_diagnostics(self._h, _ptr(uk), str(out_dir).encode(), int(iteration),
+                                             int(num_bins), ctypes.byref(d), self._stream(stream)))
+        return {"energy": d.energy, "enstrophy": d.enstrophy, "divergence_l2": d.divergence_l2}
 
     def __del__(self):
         h = getattr(self, "_h", None)

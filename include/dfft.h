@@ -219,6 +219,43 @@ dfft_status dfft_ns_step(dfft_ns* ns, void* uk, void* stream);
 /* total kinetic energy of main.cpp:746-766, (lx pi)^3 / N^2 * sum 0.5 factor |uk|^2
  * (factor 1 on kz = 0, else 2), FP64 reduction; synchronises the stream */
 dfft_status dfft_ns_energy(dfft_ns* ns, const void* uk, double* energy, void* stream);
+/* Physical velocity of a spectrum (the backward transform of diag_fields,
+ * main.cpp:711-724) into a buffer of the plan's input layout; uk is not
+ * modified. */
+dfft_status dfft_ns_velocity(dfft_ns* ns, const void* uk, void* u, void* stream);
+/* Physical vorticity curl u (compute_vorticity, main.cpp:677-698: i k x uk
+ * with the full, not dealiased, wavenumbers, then the backward transform)
+ * into a buffer of the plan's input layout; uk is not modified. */
+dfft_status dfft_ns_vorticity(dfft_ns* ns, const void* uk, void* vor, void* stream);
+/* Diagnostics of a spectrum, reduced in FP64 whatever the plan's precision:
+ *   energy         as dfft_ns_energy (main.cpp:746-766);
+ *   enstrophy      (1/2) integral |curl u|^2 = coef sum 0.5 f |k x uk|^2;
+ *   divergence_l2  (integral |div u|^2)^(1/2) = (coef sum f |k . uk|^2)^(1/2);
+ * with f = 1 on the kz = 0 plane, 2 elsewhere, coef = (lx pi)^3 / N^2.
+ * With num_bins > 0, e_spec[i] = sum of 0.5 f |uk|^2 over the modes with
+ * k_bins[i] <= |k| < k_bins[i + 1], k_bins = linspace(0, k_max, num_bins + 1)
+ * (k_max the largest |k| of the grid) and k_vals[i] the bin midpoints
+ * (diag_energy, main.cpp:471-500, :741-794; the reference uses 50 bins).
+ * num_bins <= DFFT_NS_MAX_BINS.  Synchronises the stream. */
+#define DFFT_NS_MAX_BINS 2048
+typedef struct {
+  double energy;
+  double enstrophy;
+  double divergence_l2;
+} dfft_ns_diag;
+dfft_status dfft_ns_diagnostics(dfft_ns* ns, const void* uk, int32_t num_bins, double* e_spec, double* k_vals,
+                                dfft_ns_diag* out, void* stream);
+/* The reference's diagnostic files of one iteration (diag_fields +
+ * diag_energy, main.cpp:705-818): for every virtual rank, the components of
+ * its local block of the velocity (u, v, w) and of the vorticity (vor_x,
+ * vor_y, vor_z) as raw arrays of the plan's real type in C order, named
+ * "<out_dir>/<label>_rx<rx:03>_ry<ry:03>_<iter:010>.dat" with (rx, ry) the
+ * rank's coordinates in the in_topology (1, px, py, 1); and E_spec / k_vals
+ * (num_bins doubles each) under the coordinates of rank 0.  The directory must
+ * exist.  `out` (may be NULL) receives the diagnostics of dfft_ns_diagnostics.
+ * Synchronises the stream. */
+dfft_status dfft_ns_write_diagnostics(dfft_ns* ns, const void* uk, const char* out_dir, int32_t iter,
+                                      int32_t num_bins, dfft_ns_diag* out, void* stream);
 dfft_status dfft_ns_destroy(dfft_ns* ns);
 
 /* get_all_slab_topologies (pencil = 0) / get_all_pencil_topologies (pencil = 1),

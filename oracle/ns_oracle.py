@@ -21,6 +21,11 @@ example (``examples/navier-stokes-MPI-batched/main.cpp``) and its RK4 solver
                     one ``rhs`` (main.cpp:518-528)
 * ``energy``        coef * sum 0.5 * factor * |uk|^2, factor 1 on the kz = 0 plane, else 2,
                     coef = (lx pi)^3 / N^2 (main.cpp:511-513, :746-766)
+* ``vorticity``     i k x uk with the full wavenumbers, backward transform (main.cpp:677-698)
+* ``spectrum``      radial bins linspace(0, k_max, nb + 1) over |k| (main.cpp:471-500), per bin
+                    sum 0.5 * factor * |uk|^2 with bins[i] <= |k| < bins[i + 1] (main.cpp:741-794)
+* ``enstrophy``, ``divergence_l2``  coef * sum 0.5 * factor * |k x uk|^2 and
+                    (coef * sum factor * |k . uk|^2)^(1/2): (1/2) int |curl u|^2 and (int |div u|^2)^(1/2)
 
 Transforms are numpy's pocketfft with the reference's default ``backward``
 normalisation (forward unscaled, backward scaled by 1 / N), the same
@@ -114,3 +119,51 @@ def energy(uk, lx, shape):
     factor[0] = 1.0
     e = 0.5 * factor[None, None, None, :] * (uk.real ** 2 + uk.imag ** 2)
     return float(np.sum(e) * (lx * np.pi) ** 3 / (n * n))
+
+
+def _factor(nzh):
+    f = np.full(nzh, 2.0)
+    f[0] = 1.0
+    return f[None, None, :]
+
+
+def vorticity(uk, lx, shape):
+    """Physical vorticity (3, nx, ny, nz) of the spectrum uk (compute_vorticity)."""
+    k, _, _ = wavenumbers(*shape, lx)
+    kx, ky, kz = k
+    w = np.stack([1j * (ky * uk[2] - kz * uk[1]), 1j * (kz * uk[0] - kx * uk[2]), 1j * (kx * uk[1] - ky * uk[0])])
+    return _bwd(w, shape)
+
+
+def enstrophy(uk, lx, shape):
+    nx, ny, nz = shape
+    n = float(nx) * ny * nz
+    k, _, _ = wavenumbers(*shape, lx)
+    kx, ky, kz = k
+    c = [ky * uk[2] - kz * uk[1], kz * uk[0] - kx * uk[2], kx * uk[1] - ky * uk[0]]
+    s = sum(np.abs(ci) ** 2 for ci in c)
+    return float(np.sum(0.5 * _factor(uk.shape[-1]) * s) * (lx * np.pi) ** 3 / (n * n))
+
+
+def divergence_l2(uk, lx, shape):
+    nx, ny, nz = shape
+    n = float(nx) * ny * nz
+    k, _, _ = wavenumbers(*shape, lx)
+    d = k[0] * uk[0] + k[1] * uk[1] + k[2] * uk[2]
+    return float(np.sqrt(np.sum(_factor(uk.shape[-1]) * np.abs(d) ** 2) * (lx * np.pi) ** 3 / (n * n)))
+
+
+def spectrum(uk, lx, shape, num_bins=50):
+    """(e_spec, k_vals) of diag_energy: bin edges linspace(0, k_max, nb + 1),
+    k_max the largest |k| of the grid, midpoints as k values."""
+    _, ksq, _ = wavenumbers(*shape, lx)
+    k_mag = np.sqrt(ksq)
+    k_max = float(np.max(k_mag))
+    delta = (k_max - 0.0) / num_bins
+    bins = np.array([0.0 + delta * i for i in range(num_bins)] + [k_max])
+    ek = 0.5 * _factor(uk.shape[-1]) * np.sum(np.abs(uk) ** 2, axis=0)
+    spec = np.zeros(num_bins)
+    for i in range(num_bins):
+        m = (k_mag >= bins[i]) & (k_mag < bins[i + 1])
+        spec[i] = float(np.sum(ek[m]))
+    return spec, 0.5 * (bins[:-1] + bins[1:])

@@ -127,3 +127,81 @@ def test_ns_rejects_wrong_plan():
     plan = dfft.Plan((3, 16, 16, 16), (3, 16, 16, 9), (1, 2, 3), (3, 1, 1, 1), (3, 1, 1, 1), real_input=True)
     with pytest.raises(dfft.DistributedFFTError):
         dfft.NavierStokes(plan)
+
+
+@pytest.mark.parametrize("shape,tin,tout", CASES)
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_ns_diagnostics_match_oracle(shape, tin, tout, precision):
+    """Velocity and vorticity in physical space, FP64 energy / enstrophy /
+    divergence and the 50-bin energy spectrum of a random (not projected)
+    spectrum against the oracle's restatement of main.cpp:677-794."""
+    import torch
+    lx = 2.0
+    tol = 1e-12 if precision == "float64" else 1e-5
+    plan, cdt = _setup(shape, tin, tout, precision)
+    ns = dfft.NavierStokes(plan, nu=0.01, dt=0.01, lx=lx)
+    rng = np.random.default_rng(11)
+    y = np.fft.rfftn(rng.standard_normal((3,) + shape), axes=(1, 2, 3))
+    uk = _to_dev(plan, y, cdt)
+    rdt = torch.float64 if precision == "float64" else torch.float32
+    u = torch.empty(plan.buffer_elements("in"), dtype=rdt, device="cuda")
+    ns.velocity(uk, u)
+    torch.cuda.synchronize()
+    assert _rel(dfft.gather_blocks(plan, u.cpu().numpy(), "in"), np.fft.irfftn(y, s=shape, axes=(1, 2, 3))) <= tol
+    ns.vorticity(uk, u)
+    torch.cuda.synchronize()
+    assert _rel(dfft.gather_blocks(plan, u.cpu().numpy(), "in"), N.vorticity(y, lx, shape)) <= tol
+    assert _rel(_to_host(plan, uk), y) <= (0.0 if precision == "float64" else 1e-7)  # uk not modified
+    d = ns.diagnostics(uk, num_bins=50)
+    yq = _to_host(plan, uk)  # the values the GPU saw (FP32-rounded for float32)
+    dtol = 1e-12
+    assert abs(d["energy"] / N.energy(yq, lx, shape) - 1.0) <= dtol
+    assert abs(d["enstrophy"] / N.enstrophy(yq, lx, shape) - 1.0) <= dtol
+    assert abs(d["divergence_l2"] / N.divergence_l2(yq, lx, shape) - 1.0) <= dtol
+    spec, kv = N.spectrum(yq, lx, shape, 50)
+    assert np.allclose(d["e_spec"], spec, rtol=dtol, atol=0.0)
+    assert np.array_equal(np.array(d["k_vals"]), kv)
+    # a projected field is divergence free to rounding
+    k, _, inv_ksq = N.wavenumbers(*shape, lx)
+    uk = _to_dev(plan, N.projection(y, k, inv_ksq), cdt)
+    d = ns.diagnostics(uk, num_bins=0)
+    assert d["divergence_l2"] <= (1e-12 if precision == "float64" else 1e-5) * np.sqrt(2.0 * d["enstrophy"])
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_ns_write_diagnostics_files(tmp_path, precision):
+    """The example's files: per rank (rx, ry) of in_topology (1, px, py, 1) the
+    local block of each velocity / vorticity component in C order, and the
+    spectrum under rank 0's coordinates, named label_rxNNN_ryNNN_NNNNNNNNNN.dat."""
+    import torch
+    shape, tin, tout, lx = (24, 20, 18), (1, 3, 2, 1), (1, 1, 3, 2), 2.0
+    plan, cdt = _setup(shape, tin, tout, precision)
+    ns = dfft.NavierStokes(plan, nu=0.01, dt=0.01, lx=lx)
+    uk = torch.empty(plan.buffer_elements("out"), dtype=cdt, device="cuda")
+    ns.init_taylor_green(uk)
+    d = ns.write_diagnostics(uk, tmp_path, 7, num_bins=50)
+    y = _to_host(plan, uk)
+    vel = np.fft.irfftn(y, s=shape, axes=(1, 2, 3))
+    vor = N.vorticity(y, lx, shape)
+    rdt = np.float64 if precision == "float64" else np.float32
+    tol = 1e-12 if precision == "float64" else 1e-5
+    names = set()
+    for r in range(plan.nprocs):
+        ext, st = plan.local_extents(r, "in")
+        rx, ry = r // 2, r % 2  # rank_to_coord((px, py), r), LayoutRight
+        assert (st[1], st[2]) == (sum(plan.local_extents(q * 2, "in")[0][1] for q in range(rx)),
+                                  sum(plan.local_extents(q, "in")[0][2] for q in range(ry)))
+        for field, labels in ((vel, ("u", "v", "w")), (vor, ("vor_x", "vor_y", "vor_z"))):
+            for c, lab in enumerate(labels):
+                fn = tmp_path / f"{lab}_rx{rx:03d}_ry{ry:03d}_{7:010d}.dat"
+                names.add(fn.name)
+                got = np.fromfile(fn, dtype=rdt).reshape(ext[1:])
+                ref = field[c][st[1]:st[1] + ext[1], st[2]:st[2] + ext[2], st[3]:st[3] + ext[3]]
+                assert np.max(np.abs(got - ref)) <= tol * max(1.0, np.max(np.abs(field[c])))
+    spec, kv = N.spectrum(y, lx, shape, 50)
+    assert np.allclose(np.fromfile(tmp_path / f"E_spec_rx000_ry000_{7:010d}.dat"), spec, rtol=1e-12, atol=0.0)
+    assert np.array_equal(np.fromfile(tmp_path / f"k_vals_rx000_ry000_{7:010d}.dat"), kv)
+    names |= {f"E_spec_rx000_ry000_{7:010d}.dat", f"k_vals_rx000_ry000_{7:010d}.dat"}
+    assert {p.name for p in tmp_path.iterdir()} == names
+    assert abs(d["energy"] / N.energy(y, lx, shape) - 1.0) <= 1e-12
+    assert abs(d["enstrophy"] / (3.0 * d["energy"]) - 1.0) <= tol

@@ -47,3 +47,44 @@ def test_taylor_green_decay():
         y = N.rk4_step(y, nu, dt, lx, (n, n, n))
     ratio = N.energy(y, lx, (n, n, n)) / e0
     assert abs(ratio / np.exp(-6.0 * nu * 5 * dt) - 1.0) < 1e-5
+
+
+@pytest.mark.parametrize("n,lx,v0", [(16, 2.0, 1.0), (24, 2.0, 0.5), (16, 4.0, 2.0)])
+def test_taylor_green_diagnostics(n, lx, v0):
+    """Vorticity of the vortex is v0 (-cos x sin y sin z, -sin x cos y sin z,
+    2 sin x sin y cos z) on x = lx pi i / n, so the enstrophy is 3 times the
+    energy; the field is divergence free; all its energy sits in the spectrum
+    bin of |k| = sqrt(3)."""
+    shape = (n, n, n)
+    _, uk = N.taylor_green(n, n, n, lx, v0)
+    e = N.energy(uk, lx, shape)
+    assert abs(N.enstrophy(uk, lx, shape) / (3.0 * e) - 1.0) < 1e-12
+    assert N.divergence_l2(uk, lx, shape) < 1e-12 * np.sqrt(e)
+    x = np.arange(n) * lx * np.pi / n
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    w = v0 * np.stack([-np.cos(X) * np.sin(Y) * np.sin(Z), -np.sin(X) * np.cos(Y) * np.sin(Z),
+                                    2.0 * np.sin(X) * np.sin(Y) * np.cos(Z)])
+    assert np.max(np.abs(N.vorticity(uk, lx, shape) - w)) < 1e-12 * v0
+    spec, kv = N.spectrum(uk, lx, shape, 50)
+    coef = (lx * np.pi) ** 3 / float(n ** 3) ** 2
+    assert abs(float(np.sum(spec)) * coef / e - 1.0) < 1e-12
+    kk = np.sqrt(3.0)
+    i = int(np.argmax(spec))
+    half = (kv[1] - kv[0]) / 2.0
+    assert kv[i] - half <= kk < kv[i] + half + 1e-12
+
+
+def test_spectrum_bins_follow_the_reference():
+    """Bins linspace(0, k_max, nb + 1) with the strict upper edge: the mode(s)
+    at |k| = k_max fall outside every bin, as in diag_energy."""
+    shape, lx = (8, 6, 10), 2.0
+    rng = np.random.default_rng(5)
+    uk = rng.standard_normal((3, 8, 6, 6)) + 1j * rng.standard_normal((3, 8, 6, 6))
+    spec, kv = N.spectrum(uk, lx, shape, 7)
+    _, ksq, _ = N.wavenumbers(*shape, lx)
+    km = np.sqrt(ksq)
+    f = np.full(6, 2.0)
+    f[0] = 1.0
+    ek = 0.5 * f[None, None, :] * np.sum(np.abs(uk) ** 2, axis=0)
+    assert abs(float(np.sum(spec)) - float(np.sum(ek[km < km.max()]))) < 1e-9 * float(np.sum(ek))
+    assert np.allclose(kv, (np.arange(7) + 0.5) * km.max() / 7, rtol=0, atol=1e-12)

@@ -463,7 +463,7 @@ def main():
     traffic = None  # dram bytes per launch from the committed ncu capture of this workload
     try:
         with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
-            traffic = int(json.load(f)["fft_fast_kernel_512cubed_c64"]["traffic_per_launch_bytes"])
+            traffic = int(json.load(f)["fft_stage_kernels_512cubed_c64"]["traffic_per_launch_bytes"])
     except (OSError, KeyError, ValueError):
         pass
 
@@ -488,7 +488,7 @@ def main():
             "e2e": {"value": round(world * step_bytes / (ms_e2e * 1e-3) / 1e9, 2), "unit": "GB/s",
                     "ms_per_step": round(ms_e2e, 3), "h2d_bytes_per_step": int(h_in.numel() * 8),
                     "d2h_bytes_per_step": int(h_out.numel() * 8)},
-            "roofline": {"bound": "hbm", "kernel": "fft_fast_kernel (every launch of the step: 3 axis stages per direction)",
+            "roofline": {"bound": "hbm", "kernel": "fft_pair_stream_kernel (a-fast z stages) + fft_pair_tma_kernel (TMA-fed b-fast y / x stages): every launch of the step, 3 axis stages per direction",
                          "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "algorithmic_bytes_per_launch": int(per_launch_bytes)},

@@ -251,6 +251,13 @@ dfft_status dfft_get_block_info(const dfft_plan* plan, int64_t rank, int64_t blo
   });
 }
 
+dfft_status dfft_get_device_error(const dfft_plan* plan, int32_t reset, int32_t* code) {
+  return guarded([&] {
+    if (!code) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *code = impl_of(plan).device_error(reset != 0);
+  });
+}
+
 dfft_status dfft_get_max_buffer_size(const dfft_plan* plan, uint64_t* size) {
   return guarded([&] {
     if (!size) dfft::fail(dfft::kErrInvalidArgument, "null output");

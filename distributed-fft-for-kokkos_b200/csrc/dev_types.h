@@ -52,6 +52,21 @@ struct StageArgs {
   // the same streaming tpc consecutive tiles along b per CTA
   int pairs;
   int tpc;
+  // device error word of the plan: kernels with bounded waits set it when a
+  // wait runs out (1: a TMA tile load never completed)
+  int* err;
+};
+
+// How the TMA-fed stage forms the 5 coordinates of a tile's box from the
+// tile's global coordinates: dimension d takes axis which[d] (0 b, 1 a, 2 o0,
+// 3 o1, 4 none: coordinate 0), either its position inside the rank block
+// (rank_part 0: g % lk) or its rank coordinate (rank_part 1: g / lk).  The a
+// axis is loaded in nchunks boxes of boxa positions.
+struct TmaCoords {
+  int which[5];
+  int rank_part[5];
+  int lk[5];
+  int boxa, nchunks;
 };
 
 // Per-rank geometry of one transpose, packed as int64:
@@ -106,6 +121,16 @@ int pair_stage_line_options(int n, bool afast, int* opts);
 // Lines per tile of the streaming two-line variant (A.pairs = 2).
 int pair_stage_stream_lines(int n, bool afast);
 cudaError_t launch_fft_pair(const StageArgs& A, bool inverse, bool afast, cudaStream_t st);
+// TMA-fed two-line stage (fft_tma.cu): b-fast C2C tiles of 2^k complex64
+// points (16..512) whose source is described by a tiled tensor map `map`
+// (a CUtensorMap, 128 bytes) with boxes of A.B x min(n, 256);
+// A.B must be one of pair_tma_line_options(n) and A.err a device int.
+bool pair_tma_supported(int n);
+int pair_tma_lines(int n);
+// Lines-per-tile options of the TMA stage (A.B must be one of them).
+int pair_tma_line_options(int n, int* opts);
+cudaError_t launch_fft_pair_tma(const StageArgs& A, const void* map, const TmaCoords& T, bool inverse,
+                                cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
 cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);

@@ -1,0 +1,178 @@
+// Device code of the two-complex64-lines-per-thread register stages, shared
+// by fft_pair.cu (per-thread global loads) and fft_tma.cu (TMA-fed tiles).
+// See fft_pair.cu for the thread mapping.
+#pragma once
+
+#include "fft_radix.cuh"
+
+namespace dfft {
+namespace dev {
+namespace radix {
+
+
+// One exchange of pass P for both lines of a pair: position p of the pair
+// lives at padpos(p) of the pair's shared-memory line as (x0, y0, x1, y1).
+template <int N, int P, int TT, int S>
+__device__ __forceinline__ void exchange_pair(float2* v0, float2* v1, int t, float4* line) {
+  constexpr int V = 8;
+  constexpr int R = Radix<N, P>::value, Q = V / R;
+  constexpr int R2 = Radix<N, P + 1>::value, Q2 = V / R2;
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float2 a = v0[q * R + r], b = v1[q * R + r];
+      line[padpos<S>(out_pos<N, P, TT>(t, q, r))] = make_float4(a.x, a.y, b.x, b.y);
+    }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q2; ++q)
+#pragma unroll
+    for (int r = 0; r < R2; ++r) {
+      const float4 w = line[padpos<S>(in_pos<N, P + 1, TT>(t, q, r))];
+      v0[q * R2 + r] = make_float2(w.x, w.y);
+      v1[q * R2 + r] = make_float2(w.z, w.w);
+    }
+  __syncthreads();
+}
+
+template <bool INV, int N, int P, int TT, int S>
+__device__ __forceinline__ void run_fft_pair(float2* v0, float2* v1, int t, const float2* tw, float4* line) {
+  // both lines read the same twiddles (same t): the second pass reuses them
+  compute_pass<float, INV, N, P, TT>(v0, t, tw);
+  compute_pass<float, INV, N, P, TT>(v1, t, tw);
+  if constexpr (P + 1 < Radix<N, 0>::npass) {
+    exchange_pair<N, P, TT, S>(v0, v1, t, line);
+    run_fft_pair<INV, N, P + 1, TT, S>(v0, v1, t, tw, line);
+  }
+}
+
+// Loads the pair (l0, l1) of one tile (first line b0) into v0 / v1.
+// b-fast: positions p of the pair at (line l0 offset) + p * stride; stride and
+// offsets are even (host check) and (N - 1) * stride < 2^31.
+template <int N, bool AFAST>
+__device__ __forceinline__ void load_pair(const StageArgs& A, const float2* in, int64_t so, int b0, int l0, int l1,
+                                          bool act0, bool act1, int t, float2* v0, float2* v1) {
+  using C = float2;
+  constexpr int V = 8, TT = N / V;
+  constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
+  const DevLayout& ls = A.src;
+  const C zero = make_float2(0.f, 0.f);
+  if (AFAST) {
+    const C* row0 = in + so + (act0 ? __ldg(ls.t + A.s_tb + b0 + l0) : 0);
+    const C* row1 = in + so + (act1 ? __ldg(ls.t + A.s_tb + b0 + l1) : 0);
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int p = in_pos<N, 0, TT>(t, q, r);
+        v0[q * R0 + r] = act0 ? row0[p] : zero;
+        v1[q * R0 + r] = act1 ? row1[p] : zero;
+      }
+  } else {
+    const int st = static_cast<int>(A.src_astride);
+    const int64_t base = so + (act0 ? __ldg(ls.t + A.s_tb + b0 + l0) : 0) + static_cast<int64_t>(t) * st;
+    if (act1) {
+      const float4* row = reinterpret_cast<const float4*>(in + base);
+      const int st2 = st / 2;
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+          const float4 w = row[(TT * q + r * (N / R0)) * st2];
+          v0[q * R0 + r] = make_float2(w.x, w.y);
+          v1[q * R0 + r] = make_float2(w.z, w.w);
+        }
+    } else {
+      const C* row = in + base;
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+          v0[q * R0 + r] = act0 ? row[(TT * q + r * (N / R0)) * st] : zero;
+          v1[q * R0 + r] = zero;
+        }
+    }
+  }
+}
+
+// Scales (when the stage scales) and stores the pair after the last pass.
+template <int N, bool AFAST>
+__device__ __forceinline__ void store_pair(const StageArgs& A, float2* out, int64_t dof, int b0, int l0, int l1,
+                                           bool act0, bool act1, int t, float2* v0, float2* v1) {
+  using C = float2;
+  constexpr int V = 8, TT = N / V;
+  constexpr int NPASS = Radix<N, 0>::npass;
+  constexpr int RL = Radix<N, NPASS - 1>::value, QL = V / RL;
+  const DevLayout& ld = A.dst;
+  if (A.scale != 1.0) {
+    const float s = static_cast<float>(A.scale);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      v0[e] = cscale(v0[e], s);
+      v1[e] = cscale(v1[e], s);
+    }
+  }
+  if (AFAST) {
+    C* row0 = out + dof + (act0 ? __ldg(ld.t + A.d_tb + b0 + l0) : 0);
+    C* row1 = out + dof + (act1 ? __ldg(ld.t + A.d_tb + b0 + l1) : 0);
+#pragma unroll
+    for (int q = 0; q < QL; ++q)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int p = t + last_rel<N, TT>(q, r);
+        if (act0) row0[p] = v0[q * RL + r];
+        if (act1) row1[p] = v1[q * RL + r];
+      }
+  } else if (act0) {
+    const int st = static_cast<int>(A.dst_astride);
+    const int64_t base = dof + __ldg(ld.t + A.d_tb + b0 + l0) + static_cast<int64_t>(t) * st;
+    if (act1) {
+      float4* row = reinterpret_cast<float4*>(out + base);
+      const int st2 = st / 2;
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const C a = v0[q * RL + r], b = v1[q * RL + r];
+          row[last_rel<N, TT>(q, r) * st2] = make_float4(a.x, a.y, b.x, b.y);
+        }
+    } else {
+      C* row = out + base;
+#pragma unroll
+      for (int q = 0; q < QL; ++q)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) row[last_rel<N, TT>(q, r) * st] = v0[q * RL + r];
+    }
+  }
+}
+
+
+// Line pairs per CTA, option i (0 default, 1 half, 2 double or quarter):
+//   b-fast: 8 pairs (16-line, 128-byte rows) or enough for 256 threads;
+//   a-fast: enough pairs for 128 threads;  at most 1024 threads.
+constexpr int pair_option(int n, bool afast, int i) {
+  const int tt = n / 8;
+  const int cap = 1024 / tt > 0 ? 1024 / tt : 1;
+  int p0 = afast ? (128 / tt > 1 ? 128 / tt : 1) : (256 / tt > 8 ? 256 / tt : 8);
+  if (p0 > cap) p0 = cap;
+  if (i == 0) return p0;
+  if (i == 1) return p0 / 2 > 0 ? p0 / 2 : 0;
+  if (p0 * 2 <= cap) return p0 * 2;
+  return p0 / 4 > 0 ? p0 / 4 : 0;
+}
+
+// Line pairs per CTA of the streaming variant: the default, at most 512
+// threads (about 110 registers a thread leave room for one 512-thread CTA).
+constexpr int pair_stream_pairs(int n, bool afast) {
+  const int p0 = pair_option(n, afast, 0);
+  const int cap = 512 / (n / 8) > 0 ? 512 / (n / 8) : 1;
+  return p0 < cap ? p0 : cap;
+}
+
+// b-fast tiles
+constexpr int pair_stream_pairs(int n) { return pair_stream_pairs(n, false); }
+
+}  // namespace radix
+}  // namespace dev
+}  // namespace dfft

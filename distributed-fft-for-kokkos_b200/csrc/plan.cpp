@@ -19,6 +19,8 @@
 //             for bit-exact comparison with the reference's buffers.
 #include "plan.hpp"
 
+#include <cuda.h>
+
 #include "exchange.hpp"
 
 #include <algorithm>
@@ -100,6 +102,7 @@ Plan::Plan(const PlanDesc& d, bool on_device) : d_(d), on_device_(on_device) {
       if (p) cudaFree(p);
     for (auto& kv : twiddles_) cudaFree(kv.second);
     if (d_tables_) cudaFree(d_tables_);
+    if (d_err_) cudaFree(d_err_);
     throw;
   }
 }
@@ -109,6 +112,7 @@ Plan::~Plan() {
     if (p) cudaFree(p);
   for (auto& kv : twiddles_) cudaFree(kv.second);
   if (d_tables_) cudaFree(d_tables_);
+  if (d_err_) cudaFree(d_err_);
 }
 
 void Plan::analyze() {
@@ -442,6 +446,15 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
       A.pairs = 1;
       A.B = opts[0];
       A.tiles_b = static_cast<int>((Dl.gext[b] + opts[0] - 1) / opts[0]);
+      // b-fast source tiles moved by TMA when a tensor map can describe the
+      // source layout (the default; the tuner may pick another variant)
+      const int tl = dev::pair_tma_lines(static_cast<int>(n));
+      if (!A.load_afast && tl > 0 && tma_source(src_l, A, &op.tma) && (!op.tma.b_split || op.tma.lb % tl == 0)) {
+        op.pair_B = A.B;
+        A.pairs = 3;
+        A.B = tl;
+        A.tiles_b = static_cast<int>((Dl.gext[b] + tl - 1) / tl);
+      }
     }
     const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
     if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
@@ -450,11 +463,124 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   return op;
 }
 
+// Tensor-map description of the source layout of a b-fast stage for the
+// TMA-fed kernel: dimension 0 is the tile axis b inside a rank block (unit
+// stride), then the FFT axis a, the other axes inside a block and, for every
+// split axis, its rank coordinate (stride: rank stride x block size), sorted
+// by stride; at most 5 dimensions of extent > 1.  The box is A.B lines along b
+// (set at launch) by min(n, 256) along a, so a tile lands in shared memory as
+// n rows of A.B elements.  Needs a separable layout (equal blocks) and even
+// element strides (16-byte multiples); when b is split the launch also needs
+// rank blocks a whole number of tiles wide along b (a box never crosses into
+// the next block).
+bool Plan::tma_source(int l, const dev::StageArgs& A, TmaSource* out) const {
+  const Layout& L = layouts_[l];
+  const std::size_t D = L.gext.size();
+  if (!layout_separable(L) || A.n > 1024) return false;
+  const auto blocks = layout_blocks(L);
+  const RankBlock& b0 = blocks.at(0);
+  const std::size_t a = static_cast<std::size_t>(A.a), b = static_cast<std::size_t>(A.b);
+  if (L.topo[a] != 1 || b0.stride[b] != 1 || b0.local[a] != static_cast<std::size_t>(A.n)) return false;
+  Ext rs(D, 1);
+  std::size_t acc = 1;
+  if (L.rank_right) {
+    for (long k = static_cast<long>(D) - 1; k >= 0; --k) {
+      rs[k] = acc;
+      acc *= L.topo[k];
+    }
+  } else {
+    for (std::size_t k = 0; k < D; ++k) {
+      rs[k] = acc;
+      acc *= L.topo[k];
+    }
+  }
+  struct Dim {
+    int which, rank_part;
+    std::uint64_t extent, stride, lk;
+  };
+  auto role = [&](std::size_t k) { return k == b ? 0 : k == a ? 1 : static_cast<int>(k) == A.o0 ? 2 : 3; };
+  std::vector<Dim> dims;
+  dims.push_back({0, 0, b0.local[b], 1, b0.local[b]});
+  for (std::size_t k = 0; k < D; ++k) {
+    if (k == b) continue;
+    if (b0.local[k] > 1) dims.push_back({role(k), 0, b0.local[k], b0.stride[k], b0.local[k]});
+  }
+  for (std::size_t k = 0; k < D; ++k)
+    if (L.topo[k] > 1) dims.push_back({role(k), 1, L.topo[k], rs[k] * b0.size, b0.local[k]});
+  if (dims.size() > 5) return false;
+  std::sort(dims.begin() + 1, dims.end(), [](const Dim& x, const Dim& y) { return x.stride < y.stride; });
+  TmaSource t;
+  std::uint64_t span = 16;
+  for (std::size_t d = 0; d < dims.size(); ++d) {
+    const std::uint64_t sb = dims[d].stride * 8;  // complex64
+    if (d > 0 && (sb % 16 != 0 || sb >= (std::uint64_t(1) << 40))) return false;
+    if (dims[d].extent >= (std::uint64_t(1) << 31)) return false;
+    t.dim[d] = dims[d].extent;
+    t.stride[d] = sb;
+    t.coords.which[d] = dims[d].which;
+    t.coords.rank_part[d] = dims[d].rank_part;
+    t.coords.lk[d] = static_cast<int>(dims[d].lk);
+    span = std::max(span, sb * dims[d].extent);
+  }
+  for (std::size_t d = dims.size(); d < 5; ++d) {
+    t.dim[d] = 1;
+    t.stride[d] = (span + 15) / 16 * 16;
+    t.coords.which[d] = 4;
+    t.coords.rank_part[d] = 0;
+    t.coords.lk[d] = 1;
+  }
+  const int boxa = std::min(A.n, 256);
+  for (std::size_t d = 0; d < 5; ++d) t.box[d] = 1;
+  t.lb = b0.local[b];
+  t.b_split = L.topo[b] > 1;
+  for (std::size_t d = 1; d < dims.size(); ++d)
+    if (dims[d].which == 1) t.box[d] = static_cast<std::uint32_t>(boxa);
+  t.coords.boxa = boxa;
+  t.coords.nchunks = A.n / boxa;
+  t.ok = true;
+  *out = t;
+  return true;
+}
+
 // Launch of a register-resident stage (C2C, R2C or C2R).
 static cudaError_t launch_fast_op(const dev::StageArgs& A, bool dbl, int kind, bool inverse, cudaStream_t st) {
   if (kind == dev::kR2C || kind == dev::kC2R) return dev::launch_fft_fast_real(A, dbl, kind == dev::kC2R, st);
   if (A.pairs) return dev::launch_fft_pair(A, inverse, A.load_afast != 0, st);
   return dev::launch_fft_fast(A, dbl, inverse, A.load_afast != 0, st);
+}
+
+// One stage launch with the run-time fallbacks of the two-line variants: the
+// TMA kernel needs a source the tensor map can address (16-byte aligned
+// pointer); the two-line b-fast kernels need 16-byte aligned buffers.
+cudaError_t Plan::launch_stage(const Op& op, dev::StageArgs A, cudaStream_t stream) const {
+  if (!op.fast) return dev::launch_fft_stage(A, d_.dbl, op.kind, op.inverse, op.nthreads, op.smem, op.tiles, stream);
+  const bool misaligned = ((reinterpret_cast<std::uintptr_t>(A.in) | reinterpret_cast<std::uintptr_t>(A.out)) & 15) != 0;
+  if (A.pairs == 3) {
+    alignas(64) CUtensorMap map;
+    TmaSource t = op.tma;
+    t.box[0] = static_cast<std::uint32_t>(A.B);
+    if (!misaligned && (!t.b_split || t.lb % static_cast<std::uint64_t>(A.B) == 0) && tma_encode(&map, A.in, t))
+      return dev::launch_fft_pair_tma(A, &map, t.coords, op.inverse, stream);
+    A.pairs = 1;
+    A.B = op.pair_B;
+    A.tiles_b = (A.Eb + A.B - 1) / A.B;
+  }
+  if (A.pairs && !A.load_afast && misaligned) {
+    // a caller buffer off a 16-byte boundary: the one-line kernel
+    A.pairs = 0;
+    A.B = op.single_B;
+    A.tiles_b = (A.Eb + A.B - 1) / A.B;
+  }
+  return launch_fast_op(A, d_.dbl, op.kind, op.inverse, stream);
+}
+
+int Plan::device_error(bool reset) const {
+  if (!d_err_) return 0;
+  int v = 0;
+  cuda_check(cudaDeviceSynchronize(), "device error word");
+  cuda_check(cudaMemcpy(&v, d_err_, sizeof(int), cudaMemcpyDeviceToHost), "device error word");
+  if (reset) cuda_check(cudaMemset(d_err_, 0, sizeof(int)), "device error word");
+  return v;
 }
 
 // ---------------------------------------------------------------------------
@@ -821,6 +947,11 @@ void Plan::allocate_device() {
     fail(kErrAlloc, "cudaMalloc of layout tables failed");
   }
   workspace_bytes_ += tb;
+  if (cudaMalloc(reinterpret_cast<void**>(&d_err_), sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    fail(kErrAlloc, "cudaMalloc of the device error word failed");
+  }
+  cuda_check(cudaMemset(d_err_, 0, sizeof(int)), "device error word");
   if (!host_tables_.empty())
     cuda_check(cudaMemcpy(d_tables_, host_tables_.data(), host_tables_.size() * sizeof(std::int64_t),
                           cudaMemcpyHostToDevice),
@@ -846,6 +977,7 @@ void Plan::allocate_device() {
       if (op.type == Op::Stage) {
         op.sa.src = dev_layout(op.src_layout);
         op.sa.dst = dev_layout(op.dst_layout);
+        op.sa.err = d_err_;
       } else if (op.type == Op::Pack || op.type == Op::All2All || op.type == Op::Unpack) {
         op.xa.geo = d_tables_ + reinterpret_cast<std::intptr_t>(op.xa.geo);
         if (op.type == Op::Pack) op.xa.lay = dev_layout(op.src_layout);
@@ -856,12 +988,13 @@ void Plan::allocate_device() {
 }
 
 // ---------------------------------------------------------------------------
-// Autotuner: kernel variant (one or two lines per thread) and lines per CTA
-// of every register-resident stage, timed on the
-// plan's scratch buffers at plan creation and cached per stage signature
-// (line length, precision, direction, row orientation, tile grid) for the
-// process; DFFT_TUNE_CACHE=<file> also persists the choices across processes
-// and DFFT_AUTOTUNE=0 keeps the defaults.
+// Autotuner: kernel variant (one or two lines per thread, streaming, TMA-fed)
+// and lines per CTA of every register-resident stage, timed on the plan's
+// scratch buffers at plan creation and cached per stage signature (line
+// length, precision, direction, row orientation, tile grid, the topologies of
+// both sides and the line strides) for the process; DFFT_TUNE_CACHE=<file>
+// also persists the choices across processes and DFFT_AUTOTUNE=0 keeps the
+// defaults.
 // ---------------------------------------------------------------------------
 namespace {
 std::mutex g_tune_mutex;
@@ -906,16 +1039,28 @@ void Plan::autotune() {
       std::ostringstream k;
       const bool real = op.kind == dev::kR2C || op.kind == dev::kC2R;  // two real lines per register line
       const bool pair_ok = op.single_B != 0;                            // eligible for two lines per thread
+      const bool tma_ok = op.tma.ok;                                    // eligible for the TMA-fed kernel
       k << "fast:n" << A.n << (d_.dbl ? "f64" : "f32") << (op.inverse ? "i" : "f") << (A.load_afast ? "a" : "b")
-        << (op.kind == dev::kR2C ? "r2c" : op.kind == dev::kC2R ? "c2r" : "") << (pair_ok ? "P" : "") << ":" << A.Eb
-        << "x" << A.Eo0 << "x" << A.Eo1;
+        << (op.kind == dev::kR2C ? "r2c" : op.kind == dev::kC2R ? "c2r" : "") << (pair_ok ? "P" : "")
+        << (tma_ok ? "T" : "") << ":" << A.Eb << "x" << A.Eo0 << "x" << A.Eo1;
+      // the topologies and line strides of both sides: stages of one shape
+      // that read or write differently blocked layouts are tuned apart
+      for (int side : {op.src_layout, op.dst_layout}) {
+        const Layout& Ls = layouts_[side];
+        k << ":" << (Ls.rank_right ? "R" : "L");
+        for (std::size_t t : Ls.topo) k << t << ".";
+      }
+      k << ":" << A.src_astride << "." << A.dst_astride;
       const std::string key = k.str();
       // a configuration: lines per tile of the one-line kernel; kPairCode +
       // lines per tile of the two-line kernel; kStreamCode + tiles per CTA of
-      // its streaming variant
-      constexpr int kPairCode = 100000, kStreamCode = 200000;
+      // its streaming variant; kTmaCode + lines per tile of the TMA-fed kernel
+      constexpr int kPairCode = 100000, kStreamCode = 200000, kTmaCode = 300000;
       auto apply = [&](int code) {
-        if (code >= kStreamCode) {
+        if (code >= kTmaCode) {
+          A.pairs = 3;
+          A.B = code - kTmaCode;
+        } else if (code >= kStreamCode) {
           A.pairs = 2;
           A.tpc = code - kStreamCode;
           A.B = dev::pair_stage_stream_lines(A.n, A.load_afast != 0);
@@ -927,7 +1072,7 @@ void Plan::autotune() {
         op.tiles = static_cast<unsigned>(static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1);
       };
       auto it = g_tune_cache.find(key);
-      if (it != g_tune_cache.end() && (it->second < kPairCode || pair_ok)) {
+      if (it != g_tune_cache.end() && (it->second < kPairCode || pair_ok) && (it->second < kTmaCode || tma_ok)) {
         apply(it->second);
         continue;
       }
@@ -938,6 +1083,11 @@ void Plan::autotune() {
       }
       std::vector<int> cand;
       int opts[4];
+      if (tma_ok) {
+        const int nt = dev::pair_tma_line_options(A.n, opts);
+        for (int i = 0; i < nt; ++i)
+          if (!op.tma.b_split || op.tma.lb % static_cast<std::uint64_t>(opts[i]) == 0) cand.push_back(kTmaCode + opts[i]);
+      }
       if (pair_ok) {
         const int np = dev::pair_stage_line_options(A.n, A.load_afast != 0, opts);
         for (int i = 0; i < np; ++i) cand.push_back(kPairCode + opts[i]);
@@ -948,7 +1098,7 @@ void Plan::autotune() {
       }
       const int nopt = dev::fast_stage_line_options(d_.dbl, A.n, opts);
       for (int i = 0; i < nopt; ++i) cand.push_back(opts[i]);
-      int best = A.pairs == 2 ? kStreamCode + A.tpc : (A.pairs ? kPairCode : 0) + A.B;
+      int best = A.pairs == 3 ? kTmaCode + A.B : A.pairs == 2 ? kStreamCode + A.tpc : (A.pairs ? kPairCode : 0) + A.B;
       float best_ms = std::numeric_limits<float>::max();
       cudaEvent_t e0, e1;
       cuda_check(cudaEventCreate(&e0), "tuner event");
@@ -958,12 +1108,12 @@ void Plan::autotune() {
         dev::StageArgs T = A;
         T.in = s0;
         T.out = s1;
-        if (launch_fast_op(T, d_.dbl, op.kind, op.inverse, st) != cudaSuccess) {
+        if (launch_stage(op, T, st) != cudaSuccess) {
           cudaGetLastError();
           continue;
         }
         cudaEventRecord(e0, st);
-        for (int r = 0; r < 3; ++r) launch_fast_op(T, d_.dbl, op.kind, op.inverse, st);
+        for (int r = 0; r < 3; ++r) launch_stage(op, T, st);
         cudaEventRecord(e1, st);
         cuda_check(cudaEventSynchronize(e1), "tuner sync");
         float ms = 0.f;
@@ -1001,17 +1151,7 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
         dev::StageArgs A = op0.sa;
         A.in = buf(op0.src);
         A.out = buf(op0.dst);
-        if (op0.fast && A.pairs && !A.load_afast &&
-            ((reinterpret_cast<std::uintptr_t>(A.in) | reinterpret_cast<std::uintptr_t>(A.out)) & 15)) {
-          // a caller buffer off a 16-byte boundary: the one-line kernel
-          A.pairs = 0;
-          A.B = op0.single_B;
-          A.tiles_b = (A.Eb + A.B - 1) / A.B;
-        }
-        if (op0.fast)
-          e = launch_fast_op(A, d_.dbl, op0.kind, op0.inverse, stream);
-        else
-          e = dev::launch_fft_stage(A, d_.dbl, op0.kind, op0.inverse, op0.nthreads, op0.smem, op0.tiles, stream);
+        e = launch_stage(op0, A, stream);
         break;
       }
       case Op::Pack:

@@ -30,6 +30,24 @@ struct PlanDesc {
 // Buffer ids used by the device programs.
 enum : int { kBufIn = 0, kBufOut = 1, kBufScratch0 = 2, kBufScratch1 = 3, kBufFirstDebug = 4 };
 
+// Tiled tensor-map description of a TMA-fed stage's source layout (5
+// dimensions, unused ones of extent 1): byte strides of dimensions 1..4, the
+// box, and how the kernel forms a tile's coordinates.
+struct TmaSource {
+  bool ok = false;
+  std::uint64_t lb = 0;  // extent of the tile axis b inside a rank block
+  bool b_split = false;  // b split across ranks: tiles must not cross a block
+  std::uint64_t dim[5] = {1, 1, 1, 1, 1};
+  std::uint64_t stride[5] = {0, 0, 0, 0, 0};
+  std::uint32_t box[5] = {1, 1, 1, 1, 1};
+  dev::TmaCoords coords{};
+};
+
+// Encode `t` for source address `base` into the 128-byte CUtensorMap at `map`
+// (64-byte aligned); false if the driver has no tensor-map support or refuses
+// the description (tma.cpp).
+bool tma_encode(void* map, const void* base, const TmaSource& t);
+
 struct Op {
   enum Type { Stage, Pack, All2All, Unpack, Scale, Copy, Weight } type;
   int src = -1, dst = -1;  // buffer ids
@@ -40,6 +58,9 @@ struct Op {
   bool fast = false;  // register-resident kernel (fft_fast.cu, or fft_pair.cu when sa.pairs)
   int single_B = 0;   // lines per tile of the one-line kernel, for b-fast pair stages whose
                       // caller buffers turn out not to be 16-byte aligned
+  int pair_B = 0;     // lines per tile of the two-line kernel, for TMA stages whose source
+                      // cannot be described by a tensor map at run time
+  TmaSource tma;      // source description of a TMA-eligible b-fast pair stage
   int nthreads = 256;
   std::size_t smem = 0;
   unsigned tiles = 0;
@@ -82,6 +103,8 @@ class Plan {
   std::size_t launches(bool forward) const { return prog_[forward ? 0 : 1].size(); }
   std::size_t workspace_bytes() const { return workspace_bytes_; }
   bool on_device() const { return on_device_; }
+  // Device error word (0 or the code a kernel's bounded wait left); reset clears it.
+  int device_error(bool reset) const;
   // Device tables of the caller-facing input / output layouts.
   dev::DevLayout device_layout(bool output) const;
   // Copy a buffer recorded by a capturing literal execution of transpose
@@ -114,6 +137,7 @@ class Plan {
   std::map<std::pair<int, int>, int> debug_bufs_;  // (dir, block*4 + which) -> buffer id
   int debug_buffer(int dir, std::size_t block, int which, std::size_t bytes);
   std::size_t workspace_bytes_ = 0;
+  int* d_err_ = nullptr;  // device error word (dev::StageArgs::err)
 
   void analyze();
   int add_layout(const Layout& L);
@@ -130,6 +154,8 @@ class Plan {
                         double scale, bool final_complex);
   void allocate_device();
   void autotune();
+  bool tma_source(int layout, const dev::StageArgs& A, TmaSource* out) const;
+  cudaError_t launch_stage(const Op& op, dev::StageArgs A, cudaStream_t stream) const;
   const void* twiddle(std::size_t n);
 };
 

@@ -108,6 +108,7 @@ SIGNATURES = {
     "dfft_debug_export_buffers": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
                        ctypes.c_uint64]),
+    "dfft_get_device_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "dfft_get_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
     "dfft_get_workspace_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "dfft_get_all_topologies": (

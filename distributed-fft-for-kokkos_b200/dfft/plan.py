@@ -216,6 +216,12 @@ class Plan:
         _check(lib.dfft_get_launch_count(self._h, int(direction), ctypes.byref(n)))
         return n.value
 
+    def device_error(self, reset=False):
+        """0, or the code a kernel's bounded wait left (1: a TMA tile load timed out)."""
+        c = ctypes.c_int32()
+        _check(lib.dfft_get_device_error(self._h, 1 if reset else 0, ctypes.byref(c)))
+        return c.value
+
     def workspace_bytes(self):
         n = ctypes.c_uint64()
         _check(lib.dfft_get_workspace_bytes(self._h, ctypes.byref(n)))

@@ -374,6 +374,13 @@ dfft_status dfft_propose_transpose_block(int32_t rank, const int32_t* map, const
 dfft_status dfft_debug_export_buffers(const dfft_plan* plan, int32_t direction, int64_t block, int32_t which,
                                       void* host_dst, uint64_t capacity_bytes);
 
+/* Device error word of the plan: 0, or the code a kernel left when one of
+ * its bounded waits ran out (1: a TMA tile load of a stage did not complete
+ * within about one second; that stage returned early and the transform's
+ * output is invalid).  Synchronises the device; reset = 1 clears the word.
+ * No counterpart in the reference. */
+dfft_status dfft_get_device_error(const dfft_plan* plan, int32_t reset, int32_t* code);
+
 /* Number of kernel launches one dfft_execute issues in a direction. */
 dfft_status dfft_get_launch_count(const dfft_plan* plan, int32_t direction, int64_t* launches);
 

@@ -180,6 +180,107 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def large_single_field(args, stream, barrier, max_over_ranks, gen):
+    """1024^3 FP32 C2C fwd+bwd, plain and with the compensated last radix pass,
+    their rel-L2 against the FP64 path on the same inputs; 1024^3 FP64
+    R2C / C2R fwd+bwd; Taylor-Green RK4 steps at 512^3 (FP32 and FP64), all
+    on pencils of 8 x 8 virtual ranks (the reference's perf sweep reaches
+    n = 1024)."""
+    import torch
+
+    import dfft
+
+    n = 1024
+    g = (n, n, n)
+    steps = max(3, args.steps // 10)
+    tin, tout = (8, 8, 1), (1, 8, 8)
+
+    def time_pair(plan, a, b, c, k):
+        for _ in range(args.warmup):
+            dfft.execute(plan, a, b, dfft.Direction.forward)
+            dfft.execute(plan, b, c, dfft.Direction.backward)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            dfft.execute(plan, a, b, dfft.Direction.forward)
+            dfft.execute(plan, b, c, dfft.Direction.backward)
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / k)
+
+    res = {"n": n, "topology_in": list(tin), "topology_out": list(tout), "timed_steps": steps}
+    x = torch.randn(n ** 3, dtype=torch.complex64, device="cuda", generator=gen)
+    outs = {}
+    for prec in ("float32", "float32_compensated"):
+        p = dfft.Plan(g, g, (0, 1, 2), tin, tout, precision=prec, stream=stream.cuda_stream)
+        y = torch.empty_like(x)
+        z = torch.empty_like(x)
+        ms = time_pair(p, x, y, z, steps)
+        dfft.execute(p, x, y, dfft.Direction.forward)
+        key = "fp32" if prec == "float32" else "fp32_compensated"
+        res[key + "_ms_per_fwd_bwd"] = round(ms, 4)
+        res[key + "_GBps"] = round(algo_bytes(n, 8) / (ms * 1e-3) / 1e9, 1)
+        outs[key] = y
+        del p, z
+        torch.cuda.empty_cache()
+    peak, _ = measured_peak()
+    res["fp32_frac_of_measured_hbm"] = round(res["fp32_GBps"] / peak, 4)
+    p64 = dfft.Plan(g, g, (0, 1, 2), tin, tout, precision="float64", stream=stream.cuda_stream)
+    y64 = torch.empty(n ** 3, dtype=torch.complex128, device="cuda")
+    dfft.execute(p64, x.to(torch.complex128), y64, dfft.Direction.forward)
+    torch.cuda.synchronize()
+    nrm = torch.linalg.vector_norm(y64)
+    for key, y in outs.items():
+        res["rel_l2_" + key + "_vs_fp64"] = float(torch.linalg.vector_norm(y.to(torch.complex128) - y64) / nrm)
+    del p64, y64, outs, x
+    torch.cuda.empty_cache()
+    # FP64 R2C / C2R
+    pr = dfft.Plan(g, (n, n, n // 2 + 1), (0, 1, 2), tin, tout, real_input=True, precision="float64",
+                   stream=stream.cuda_stream)
+    xr = torch.randn(n ** 3, dtype=torch.float64, device="cuda", generator=gen)
+    yr = torch.empty(pr.buffer_elements("out"), dtype=torch.complex128, device="cuda")
+    zr = torch.empty_like(xr)
+    ms = time_pair(pr, xr, yr, zr, max(3, steps // 2))
+    res["fp64_r2c_c2r_ms_per_fwd_bwd"] = round(ms, 4)
+    # per direction: the real field once, the half spectrum (n^2 (n/2+1)) five
+    # times (R2C write, then read + write of the two C2C stages)
+    res["fp64_r2c_c2r_GBps"] = round(2 * (n ** 3 * 8 + 5 * n * n * (n // 2 + 1) * 16) / (ms * 1e-3) / 1e9, 1)
+    res["fp64_r2c_c2r_roundtrip_rel_l2"] = float(torch.linalg.vector_norm(zr - xr) / torch.linalg.vector_norm(xr))
+    del pr, xr, yr, zr
+    torch.cuda.empty_cache()
+    # Taylor-Green at 512^3, Re 1600, dt 1e-3
+    m = 512
+    tg = {"n": m, "re": 1600, "dt": 1e-3, "topology_in": [1, 8, 8, 1], "topology_out": [1, 1, 8, 8]}
+    energies = {}
+    for prec in ("float32", "float64"):
+        pl = dfft.Plan((3, m, m, m), (3, m, m, m // 2 + 1), (1, 2, 3), (1, 8, 8, 1), (1, 1, 8, 8), real_input=True,
+                       precision=prec, stream=stream.cuda_stream)
+        st = dfft.NavierStokes(pl, nu=1.0 / 1600.0, dt=1e-3, lx=2.0)
+        uk = torch.empty(pl.buffer_elements("out"), dtype=torch.complex64 if prec == "float32" else torch.complex128,
+                         device="cuda")
+        st.init_taylor_green(uk, stream=stream.cuda_stream)
+        e0 = st.energy(uk, stream=stream.cuda_stream)
+        st.step(uk, stream=stream.cuda_stream)
+        barrier()
+        k = 4
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(k):
+            st.step(uk, stream=stream.cuda_stream)
+        t1.record(stream)
+        barrier()
+        tg[prec + "_ms_per_rk4_step"] = round(max_over_ranks(t0.elapsed_time(t1) / k), 3)
+        energies[prec] = st.energy(uk, stream=stream.cuda_stream) / e0
+        del st, pl, uk
+        torch.cuda.empty_cache()
+    tg["energy_ratio_after_5_steps_fp64"] = energies["float64"]
+    tg["rel_diff_energy_fp32_vs_fp64"] = abs(energies["float32"] / energies["float64"] - 1.0)
+    tg["fp32_over_fp64_speedup"] = round(tg["float64_ms_per_rk4_step"] / tg["float32_ms_per_rk4_step"], 3)
+    res["taylor_green_512"] = tg
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -454,6 +555,13 @@ def main():
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
 
+    # ---- large single field: 1024^3 FP32 C2C (plain and compensated last
+    # pass) and 1024^3 FP64 R2C / C2R on a pencil of 8 x 8 virtual ranks, and
+    # the Taylor-Green vortex at 512^3 (FP32 and FP64 RK4 steps) ----
+    del a32, b32, c32, graph, p32
+    torch.cuda.empty_cache()
+    large = large_single_field(args, stream, barrier, max_over_ranks, gen)
+
     step_bytes = algo_bytes(n, 8)
     value = world * step_bytes / (ms32 * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
@@ -481,6 +589,7 @@ def main():
                                "speedup": round(ms_batch64 / ms_batch32, 3),
                                "fp32_graph_GBps": round(batch_bytes / (ms_batch32 * 1e-3) / 1e9, 1)},
             "navier_stokes_batch16": ns_res,
+            "large_single_field": large,
             "fp64_ms_per_step": round(ms64, 4),
             "fp32_over_fp64_speedup": round(ms64 / ms32, 3),
             "rel_l2_fp32_vs_fp64_forward": err_fwd,

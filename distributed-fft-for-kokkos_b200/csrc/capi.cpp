@@ -75,12 +75,13 @@ dfft::PlanDesc to_desc(const dfft_plan_desc* d) {
   p.out_right = d->out_topology_layout_right != 0;
   p.view_right = d->view_layout_right != 0;
   if (d->kind != DFFT_KIND_C2C && d->kind != DFFT_KIND_R2C) dfft::fail(dfft::kErrInvalidArgument, "unknown kind");
-  if (d->precision != DFFT_PREC_F64 && d->precision != DFFT_PREC_F32)
+  if (d->precision != DFFT_PREC_F64 && d->precision != DFFT_PREC_F32 && d->precision != DFFT_PREC_F32_COMPENSATED)
     dfft::fail(dfft::kErrInvalidArgument, "unknown precision");
   if (d->exec_mode != DFFT_EXEC_FUSED && d->exec_mode != DFFT_EXEC_LITERAL && d->exec_mode != DFFT_EXEC_LITERAL_CAPTURE)
     dfft::fail(dfft::kErrInvalidArgument, "unknown execution mode");
   p.r2c = d->kind == DFFT_KIND_R2C;
   p.dbl = d->precision == DFFT_PREC_F64;
+  p.comp = d->precision == DFFT_PREC_F32_COMPENSATED;
   p.norm = d->normalization;
   p.exec_mode = d->exec_mode;
   p.stream = static_cast<cudaStream_t>(d->stream);

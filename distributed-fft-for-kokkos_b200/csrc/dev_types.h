@@ -55,6 +55,9 @@ struct StageArgs {
   // device error word of the plan: kernels with bounded waits set it when a
   // wait runs out (1: a TMA tile load never completed)
   int* err;
+  // two-line kernels: 1 = last radix pass in compensated arithmetic (the
+  // default tile of fft_pair_kernel and of the TMA kernel only)
+  int comp;
 };
 
 // How the TMA-fed stage forms the 5 coordinates of a tile's box from the

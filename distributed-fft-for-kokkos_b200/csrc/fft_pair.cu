@@ -22,15 +22,19 @@ using namespace radix;
 namespace {
 
 // 1024 resident threads per SM: 64 registers for 16 complex64 values a thread
-template <int THREADS>
+// (the compensated variant, with twice the live values in its last pass,
+// keeps the compiler's choice)
+template <int THREADS, bool COMP>
 struct PairMinBlocks {
   static constexpr int v = 1024 / THREADS;
-  static constexpr int value = v > 0 ? v : 1;
+  static constexpr int value = (v > 0 && !COMP) ? v : 1;
 };
 
-// PB line pairs per CTA (2 PB lines), N/8 threads per pair.
-template <bool INV, int N, int PB, bool AFAST>
-__global__ void __launch_bounds__(N / 8 * PB, (PairMinBlocks<N / 8 * PB>::value)) fft_pair_kernel(const StageArgs A) {
+// PB line pairs per CTA (2 PB lines), N/8 threads per pair.  COMP: the last
+// radix pass in compensated arithmetic (compute_pass_comp).
+template <bool INV, int N, int PB, bool AFAST, bool COMP = false>
+__global__ void __launch_bounds__(N / 8 * PB, (PairMinBlocks<N / 8 * PB, COMP>::value))
+    fft_pair_kernel(const StageArgs A) {
   using C = float2;
   constexpr int V = 8;
   static_assert(Vals<N>::value == V, "two-line kernel: lines of 2^k points");
@@ -75,7 +79,7 @@ __global__ void __launch_bounds__(N / 8 * PB, (PairMinBlocks<N / 8 * PB>::value)
   load_pair<N, AFAST>(A, in, so, b0, l0, l1, act0, act1, t, v0, v1);
   __syncthreads();  // twiddles staged
 
-  run_fft_pair<INV, N, 0, TT, SH::S>(v0, v1, t, tw, tile + lp * LP);
+  run_fft_pair<INV, N, 0, TT, SH::S, COMP>(v0, v1, t, tw, tile + lp * LP);
 
   store_pair<N, AFAST>(A, reinterpret_cast<C*>(A.out), dof, b0, l0, l1, act0, act1, t, v0, v1);
 }
@@ -146,14 +150,14 @@ __global__ void __launch_bounds__(N / 8 * PB, 1) fft_pair_stream_kernel(const St
   }
 }
 
-template <int N, bool INV, bool AF, int PB>
+template <int N, bool INV, bool AF, int PB, bool COMP = false>
 static cudaError_t launch_pair_b(const StageArgs& A, cudaStream_t st) {
   if constexpr (PB <= 0) {
     return cudaErrorInvalidValue;
   } else {
     constexpr int LP = SmemShape<double, N, PB, AF>::LP;
     const size_t smem = sizeof(float2) * N + sizeof(float4) * static_cast<size_t>(PB) * LP;
-    auto k = fft_pair_kernel<INV, N, PB, AF>;
+    auto k = fft_pair_kernel<INV, N, PB, AF, COMP>;
     const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     k<<<fast_grid(A), N / 8 * PB, smem, st>>>(with_table_offsets(A));
@@ -179,6 +183,7 @@ static cudaError_t launch_pair_stream(const StageArgs& A, cudaStream_t st) {
 template <int N, bool INV, bool AF>
 static cudaError_t launch_pair_n(const StageArgs& A, cudaStream_t st) {
   constexpr int P0 = pair_option(N, AF, 0), P1 = pair_option(N, AF, 1), P2 = pair_option(N, AF, 2);
+  if (A.comp) return A.B == 2 * P0 ? launch_pair_b<N, INV, AF, P0, true>(A, st) : cudaErrorInvalidValue;
   if (A.B == 2 * P0) return launch_pair_b<N, INV, AF, P0>(A, st);
   if (P1 > 0 && A.B == 2 * P1) return launch_pair_b<N, INV, AF, P1>(A, st);
   if (P2 > 0 && A.B == 2 * P2) return launch_pair_b<N, INV, AF, P2>(A, st);
@@ -188,6 +193,7 @@ static cudaError_t launch_pair_n(const StageArgs& A, cudaStream_t st) {
 template <int N>
 static cudaError_t launch_pair_t(const StageArgs& A, bool inverse, bool afast, cudaStream_t st) {
   if (A.pairs == 2) {
+    if (A.comp) return cudaErrorInvalidValue;
     if (inverse) return afast ? launch_pair_stream<N, true, true>(A, st) : launch_pair_stream<N, true, false>(A, st);
     return afast ? launch_pair_stream<N, false, true>(A, st) : launch_pair_stream<N, false, false>(A, st);
   }

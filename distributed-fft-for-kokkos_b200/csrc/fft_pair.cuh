@@ -36,14 +36,26 @@ __device__ __forceinline__ void exchange_pair(float2* v0, float2* v1, int t, flo
   __syncthreads();
 }
 
-template <bool INV, int N, int P, int TT, int S>
+// One radix pass of both lines: the compensated variant for the last pass
+// when COMP is set.
+template <bool INV, int N, int P, int TT, bool COMP>
+__device__ __forceinline__ void pass_pair(float2* v0, float2* v1, int t, const float2* tw) {
+  if constexpr (COMP && P + 1 == Radix<N, 0>::npass) {
+    compute_pass_comp<INV, N, P, TT>(v0, t, tw);
+    compute_pass_comp<INV, N, P, TT>(v1, t, tw);
+  } else {
+    // both lines read the same twiddles (same t): the second pass reuses them
+    compute_pass<float, INV, N, P, TT>(v0, t, tw);
+    compute_pass<float, INV, N, P, TT>(v1, t, tw);
+  }
+}
+
+template <bool INV, int N, int P, int TT, int S, bool COMP = false>
 __device__ __forceinline__ void run_fft_pair(float2* v0, float2* v1, int t, const float2* tw, float4* line) {
-  // both lines read the same twiddles (same t): the second pass reuses them
-  compute_pass<float, INV, N, P, TT>(v0, t, tw);
-  compute_pass<float, INV, N, P, TT>(v1, t, tw);
+  pass_pair<INV, N, P, TT, COMP>(v0, v1, t, tw);
   if constexpr (P + 1 < Radix<N, 0>::npass) {
     exchange_pair<N, P, TT, S>(v0, v1, t, line);
-    run_fft_pair<INV, N, P + 1, TT, S>(v0, v1, t, tw, line);
+    run_fft_pair<INV, N, P + 1, TT, S, COMP>(v0, v1, t, tw, line);
   }
 }
 

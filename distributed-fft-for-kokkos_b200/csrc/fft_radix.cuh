@@ -209,6 +209,121 @@ __device__ __forceinline__ void compute_pass(cplx<T>* v, int t, const cplx<T>* t
   }
 }
 
+// ---- Compensated final radix-8 pass (complex64) ----
+// Each value of the pass is carried as an unevaluated sum hi + lo of two
+// floats: the twiddle products are split exactly with fused multiply-adds
+// (p = a b rounded, e = fma(a, b, -p) = a b - p exactly), every addition of
+// the butterfly is an error-free two-sum (Knuth: s = a + b rounded,
+// e = (a - (s - (s - a))) + (b - (s - a)) = a + b - s exactly) whose error
+// term is carried in lo, the 1/sqrt(2) rotations use a two-float constant,
+// and each output is rounded once, hi + lo.  The intrinsics (__fadd_rn,
+// __fmul_rn) keep the compiler from contracting the additions and products
+// into fused multiply-adds, which would break the error-free identities.
+// All seven twiddles are read from the table (no products of twiddles).
+struct DFloat {
+  float hi, lo;
+};
+struct DCplx {
+  DFloat x, y;
+};
+
+__device__ __forceinline__ DFloat two_sum(float a, float b) {
+  const float s = __fadd_rn(a, b);
+  const float bb = __fadd_rn(s, -a);
+  const float e = __fadd_rn(__fadd_rn(a, -__fadd_rn(s, -bb)), __fadd_rn(b, -bb));
+  return DFloat{s, e};
+}
+__device__ __forceinline__ DFloat df_add(DFloat a, DFloat b) {
+  DFloat r = two_sum(a.hi, b.hi);
+  r.lo = __fadd_rn(r.lo, __fadd_rn(a.lo, b.lo));
+  return r;
+}
+__device__ __forceinline__ DFloat df_neg(DFloat a) { return DFloat{-a.hi, -a.lo}; }
+__device__ __forceinline__ DFloat df_sub(DFloat a, DFloat b) { return df_add(a, df_neg(b)); }
+__device__ __forceinline__ DCplx dc_add(DCplx a, DCplx b) { return DCplx{df_add(a.x, b.x), df_add(a.y, b.y)}; }
+__device__ __forceinline__ DCplx dc_sub(DCplx a, DCplx b) { return DCplx{df_sub(a.x, b.x), df_sub(a.y, b.y)}; }
+// s i z, s = -1 forward, +1 inverse (exact)
+template <bool INV>
+__device__ __forceinline__ DCplx dc_rot(DCplx z) {
+  return INV ? DCplx{df_neg(z.y), z.x} : DCplx{z.y, df_neg(z.x)};
+}
+// a * (1/sqrt 2) with the constant as the two floats kH + kHl
+__device__ __forceinline__ DFloat df_mul_h(DFloat a) {
+  constexpr double hd = 0.70710678118654752440084436210484903928;
+  constexpr float kH = static_cast<float>(hd);
+  constexpr float kHl = static_cast<float>(hd - static_cast<double>(kH));
+  const float p = __fmul_rn(a.hi, kH);
+  const float pe = __fmaf_rn(a.hi, kH, -p);
+  return DFloat{p, __fadd_rn(pe, __fadd_rn(__fmul_rn(a.lo, kH), __fmul_rn(a.hi, kHl)))};
+}
+// exact product of two complex64 values as hi + lo pairs
+__device__ __forceinline__ DCplx dc_mul_exact(float2 v, float2 w) {
+  float p = __fmul_rn(v.x, w.x), pe = __fmaf_rn(v.x, w.x, -p);
+  float q = __fmul_rn(v.y, w.y), qe = __fmaf_rn(v.y, w.y, -q);
+  DCplx r;
+  r.x = two_sum(p, -q);
+  r.x.lo = __fadd_rn(r.x.lo, __fadd_rn(pe, -qe));
+  p = __fmul_rn(v.x, w.y);
+  pe = __fmaf_rn(v.x, w.y, -p);
+  q = __fmul_rn(v.y, w.x);
+  qe = __fmaf_rn(v.y, w.x, -q);
+  r.y = two_sum(p, q);
+  r.y.lo = __fadd_rn(r.y.lo, __fadd_rn(pe, qe));
+  return r;
+}
+
+template <bool INV>
+__device__ __forceinline__ void dc_r4(DCplx& v0, DCplx& v1, DCplx& v2, DCplx& v3) {
+  const DCplx s02 = dc_add(v0, v2), d02 = dc_sub(v0, v2);
+  const DCplx s13 = dc_add(v1, v3), d13 = dc_rot<INV>(dc_sub(v1, v3));
+  v0 = dc_add(s02, s13);
+  v2 = dc_sub(s02, s13);
+  v1 = dc_add(d02, d13);
+  v3 = dc_sub(d02, d13);
+}
+
+// Final radix-8 pass P (twiddled, Ns = N / 8 > 1) of one line in compensated
+// arithmetic; same data movement as compute_pass.
+template <bool INV, int N, int P, int TT>
+__device__ __forceinline__ void compute_pass_comp(float2* v, int t, const float2* tw) {
+  constexpr int R = Radix<N, P>::value;
+  constexpr int Ns = NsOf<N, P>::value;
+  static_assert(R == 8 && Vals<N>::value == 8, "compensated pass: radix 8, 8 values per thread");
+  DCplx d[8];
+  d[0] = DCplx{DFloat{v[0].x, 0.f}, DFloat{v[0].y, 0.f}};
+  if (Ns > 1) {
+    const int k = t % Ns;
+    const int m = k * (N / (Ns * R));
+#pragma unroll
+    for (int r = 1; r < 8; ++r) {
+      float2 w = tw[r * m];
+      if (INV) w.y = -w.y;
+      d[r] = dc_mul_exact(v[r], w);
+    }
+  } else {
+#pragma unroll
+    for (int r = 1; r < 8; ++r) d[r] = DCplx{DFloat{v[r].x, 0.f}, DFloat{v[r].y, 0.f}};
+  }
+  DCplx e0 = d[0], e1 = d[2], e2 = d[4], e3 = d[6];
+  DCplx o0 = d[1], o1 = d[3], o2 = d[5], o3 = d[7];
+  dc_r4<INV>(e0, e1, e2, e3);
+  dc_r4<INV>(o0, o1, o2, o3);
+  DCplx t1, t3;
+  if (INV) {
+    t1 = DCplx{df_mul_h(df_sub(o1.x, o1.y)), df_mul_h(df_add(o1.x, o1.y))};
+    t3 = DCplx{df_neg(df_mul_h(df_add(o3.x, o3.y))), df_mul_h(df_sub(o3.x, o3.y))};
+  } else {
+    t1 = DCplx{df_mul_h(df_add(o1.x, o1.y)), df_mul_h(df_sub(o1.y, o1.x))};
+    t3 = DCplx{df_mul_h(df_sub(o3.y, o3.x)), df_neg(df_mul_h(df_add(o3.x, o3.y)))};
+  }
+  const DCplx t2 = dc_rot<INV>(o2);
+  const DCplx out[8] = {dc_add(e0, o0), dc_add(e1, t1), dc_add(e2, t2), dc_add(e3, t3),
+                        dc_sub(e0, o0), dc_sub(e1, t1), dc_sub(e2, t2), dc_sub(e3, t3)};
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+    v[r] = make_float2(__fadd_rn(out[r].x.hi, out[r].x.lo), __fadd_rn(out[r].y.hi, out[r].y.lo));
+}
+
 template <typename T, bool INV, int N, int P, int TT, int S>
 __device__ __forceinline__ void exchange(cplx<T>* v, int t, cplx<T>* line) {
   constexpr int V = Vals<N>::value;

@@ -179,13 +179,12 @@ __device__ __forceinline__ void exchange_dense(float2* v0, float2* v1, int t, fl
   __syncthreads();
 }
 
-template <bool INV, int N, int P, int TT, int PB>
+template <bool INV, int N, int P, int TT, int PB, bool COMP>
 __device__ __forceinline__ void run_fft_dense(float2* v0, float2* v1, int t, const float2* tw, float4* buf) {
-  compute_pass<float, INV, N, P, TT>(v0, t, tw);
-  compute_pass<float, INV, N, P, TT>(v1, t, tw);
+  pass_pair<INV, N, P, TT, COMP>(v0, v1, t, tw);
   if constexpr (P + 1 < Radix<N, 0>::npass) {
     exchange_dense<N, P, TT, PB>(v0, v1, t, buf);
-    run_fft_dense<INV, N, P + 1, TT, PB>(v0, v1, t, tw, buf);
+    run_fft_dense<INV, N, P + 1, TT, PB, COMP>(v0, v1, t, tw, buf);
   }
 }
 
@@ -249,7 +248,7 @@ struct TmaMinBlocks {
   static constexpr int value = v > 0 ? v : 1;
 };
 
-template <bool INV, int N, int PB>
+template <bool INV, int N, int PB, bool COMP>
 __global__ void __launch_bounds__(N / 8 * PB, (TmaMinBlocks<N, PB>::value))
     fft_pair_tma_kernel(const __grid_constant__ CUtensorMap map, const StageArgs A, const TmaCoords T) {
   using C = float2;
@@ -331,7 +330,7 @@ __global__ void __launch_bounds__(N / 8 * PB, (TmaMinBlocks<N, PB>::value))
       }
       return;
     }
-    run_fft_dense<INV, N, 0, TT, PB>(v0, v1, t, tw, reinterpret_cast<float4*>(buf) + lp);  // ends on a barrier
+    run_fft_dense<INV, N, 0, TT, PB, COMP>(v0, v1, t, tw, reinterpret_cast<float4*>(buf) + lp);  // ends on a barrier
     if (threadIdx.x == 0 && issued < ntiles) {
       fence_proxy_async();
       issue_tile<N, L>(&map, T, nxt.tb, nxt.co0, nxt.co1, buf, bars + s);
@@ -347,14 +346,14 @@ __global__ void __launch_bounds__(N / 8 * PB, (TmaMinBlocks<N, PB>::value))
   }
 }
 
-template <int N, bool INV, int PB>
+template <int N, bool INV, int PB, bool COMP = false>
 cudaError_t launch_tma_pb(const StageArgs& A, const void* map, const TmaCoords& T, cudaStream_t st) {
   if constexpr (PB < 1) {
     return cudaErrorInvalidValue;
   } else {
     constexpr size_t smem = tma_smem_bytes<N, PB>();
     static_assert(smem <= 227 * 1024, "TMA stage tiles do not fit in shared memory");
-    auto k = fft_pair_tma_kernel<INV, N, PB>;
+    auto k = fft_pair_tma_kernel<INV, N, PB, COMP>;
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0, sms = 0, dev = 0;
@@ -383,6 +382,8 @@ constexpr int tma_pairs(int n, int i) {
 
 template <int N, bool INV>
 cudaError_t launch_tma_n(const StageArgs& A, const void* map, const TmaCoords& T, cudaStream_t st) {
+  if (A.comp) return A.B == 2 * tma_pairs(N, 0) ? launch_tma_pb<N, INV, tma_pairs(N, 0), true>(A, map, T, st)
+                                                 : cudaErrorInvalidValue;
   if (A.B == 2 * tma_pairs(N, 0)) return launch_tma_pb<N, INV, tma_pairs(N, 0)>(A, map, T, st);
   if (A.B == 2 * tma_pairs(N, 1)) return launch_tma_pb<N, INV, tma_pairs(N, 1)>(A, map, T, st);
   return cudaErrorInvalidValue;

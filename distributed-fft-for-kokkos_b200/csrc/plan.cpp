@@ -455,6 +455,8 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
         A.B = tl;
         A.tiles_b = static_cast<int>((Dl.gext[b] + tl - 1) / tl);
       }
+      // compensated last pass: the default tiles of the two kernels above
+      if (d_.comp) A.comp = 1;
     }
     const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
     if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
@@ -566,8 +568,10 @@ cudaError_t Plan::launch_stage(const Op& op, dev::StageArgs A, cudaStream_t stre
     A.tiles_b = (A.Eb + A.B - 1) / A.B;
   }
   if (A.pairs && !A.load_afast && misaligned) {
-    // a caller buffer off a 16-byte boundary: the one-line kernel
+    // a caller buffer off a 16-byte boundary: the one-line kernel (plain
+    // FP32 arithmetic)
     A.pairs = 0;
+    A.comp = 0;
     A.B = op.single_B;
     A.tiles_b = (A.Eb + A.B - 1) / A.B;
   }
@@ -1042,7 +1046,7 @@ void Plan::autotune() {
       const bool tma_ok = op.tma.ok;                                    // eligible for the TMA-fed kernel
       k << "fast:n" << A.n << (d_.dbl ? "f64" : "f32") << (op.inverse ? "i" : "f") << (A.load_afast ? "a" : "b")
         << (op.kind == dev::kR2C ? "r2c" : op.kind == dev::kC2R ? "c2r" : "") << (pair_ok ? "P" : "")
-        << (tma_ok ? "T" : "") << ":" << A.Eb << "x" << A.Eo0 << "x" << A.Eo1;
+        << (tma_ok ? "T" : "") << (A.comp ? "C" : "") << ":" << A.Eb << "x" << A.Eo0 << "x" << A.Eo1;
       // the topologies and line strides of both sides: stages of one shape
       // that read or write differently blocked layouts are tuned apart
       for (int side : {op.src_layout, op.dst_layout}) {
@@ -1083,12 +1087,17 @@ void Plan::autotune() {
       }
       std::vector<int> cand;
       int opts[4];
-      if (tma_ok) {
+      if (A.comp) {
+        // compensated stages: the default tiles of the TMA and two-line kernels
+        if (tma_ok) cand.push_back(kTmaCode + dev::pair_tma_lines(A.n));
+        dev::pair_stage_line_options(A.n, A.load_afast != 0, opts);
+        cand.push_back(kPairCode + opts[0]);
+      } else if (tma_ok) {
         const int nt = dev::pair_tma_line_options(A.n, opts);
         for (int i = 0; i < nt; ++i)
           if (!op.tma.b_split || op.tma.lb % static_cast<std::uint64_t>(opts[i]) == 0) cand.push_back(kTmaCode + opts[i]);
       }
-      if (pair_ok) {
+      if (pair_ok && !A.comp) {
         const int np = dev::pair_stage_line_options(A.n, A.load_afast != 0, opts);
         for (int i = 0; i < np; ++i) cand.push_back(kPairCode + opts[i]);
         const int sb = dev::pair_stage_stream_lines(A.n, A.load_afast != 0);
@@ -1096,7 +1105,7 @@ void Plan::autotune() {
         for (int tpc : {4, 8, 16})
           if (tiles >= 2 * tpc) cand.push_back(kStreamCode + tpc);
       }
-      const int nopt = dev::fast_stage_line_options(d_.dbl, A.n, opts);
+      const int nopt = A.comp ? 0 : dev::fast_stage_line_options(d_.dbl, A.n, opts);
       for (int i = 0; i < nopt; ++i) cand.push_back(opts[i]);
       int best = A.pairs == 3 ? kTmaCode + A.B : A.pairs == 2 ? kStreamCode + A.tpc : (A.pairs ? kPairCode : 0) + A.B;
       float best_ms = std::numeric_limits<float>::max();

@@ -22,6 +22,7 @@ struct PlanDesc {
   bool in_right = true, out_right = true, view_right = true;
   bool r2c = false;
   bool dbl = true;
+  bool comp = false;  // FP32 with the compensated last radix pass of two-line stages
   int norm = 0;       // 0 backward, 1 forward, 2 ortho, 3 none
   int exec_mode = 0;  // 0 fused, 1 literal, 2 literal with capture of every exchange
   cudaStream_t stream = nullptr;

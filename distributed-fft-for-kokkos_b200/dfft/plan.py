@@ -89,7 +89,8 @@ class Plan:
       axes : FFT axes (1 to 3; negative values count from the end)
       in_topology / out_topology : ranks along each axis
       real_input : R2C forward / C2R backward plan (else C2C)
-      precision : "float64" or "float32"
+      precision : "float64", "float32" or "float32_compensated" (complex64 with
+                  the last radix pass of the two-line C2C stages compensated)
       norm : Normalization (default backward)
       layout : memory order of the local blocks, "right" (C) or "left" (Fortran)
       in_topology_layout / out_topology_layout : rank order of the topologies
@@ -124,9 +125,9 @@ class Plan:
         d.out_topology_layout_right = 1 if out_topology_layout == "right" else 0
         d.view_layout_right = 1 if layout == "right" else 0
         d.kind = 1 if real_input else 0
-        if precision not in ("float64", "float32"):
+        if precision not in ("float64", "float32", "float32_compensated"):
             raise DistributedFFTError(Status.INVALID_ARGUMENT, f"unknown precision {precision}")
-        d.precision = 0 if precision == "float64" else 1
+        d.precision = {"float64": 0, "float32": 1, "float32_compensated": 2}[precision]
         d.normalization = int(_as_norm(norm))
         d.exec_mode = int(ExecMode[exec_mode] if isinstance(exec_mode, str) else exec_mode)
         d.stream = ctypes.c_void_p(int(stream)) if stream else None

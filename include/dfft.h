@@ -51,8 +51,15 @@ typedef enum {
 /* Transform kind.  R2C plans run C2R on dfft_execute(..., DFFT_BACKWARD). */
 typedef enum { DFFT_KIND_C2C = 0, DFFT_KIND_R2C = 1 } dfft_kind;
 
-/* Storage and arithmetic precision: complex128/float64 or complex64/float32. */
-typedef enum { DFFT_PREC_F64 = 0, DFFT_PREC_F32 = 1 } dfft_precision;
+/* Storage and arithmetic precision: complex128/float64 or complex64/float32.
+ * DFFT_PREC_F32_COMPENSATED stores and computes like DFFT_PREC_F32, except
+ * that the last radix pass of every two-line C2C stage (power-of-two lines
+ * on 16-byte aligned buffers: the stages of 3D C2C pencils and slabs) runs in
+ * compensated arithmetic: exact twiddle products through fused multiply-adds,
+ * error-free two-sum additions carried as hi + lo float pairs, one rounding
+ * per output.  Other stages run the plain FP32 kernels.  No counterpart in the
+ * reference (which has no FP32 path with compensation). */
+typedef enum { DFFT_PREC_F64 = 0, DFFT_PREC_F32 = 1, DFFT_PREC_F32_COMPENSATED = 2 } dfft_precision;
 
 /* KokkosFFT::Normalization (default backward: 1/N on the backward transform). */
 typedef enum {

@@ -53,3 +53,26 @@ def test_tma_stage_layout_left(monkeypatch):
     X = run(plan, x, True)
     assert O.rel_l2(X, O.global_fft(x, (0, 1, 2), False)) <= 1e-6
     assert plan.device_error() == 0
+
+
+@pytest.mark.parametrize("gin,tin,tout", [
+    ((256, 256, 256), (4, 4, 1), (1, 4, 4)),   # a-fast z stage + TMA-fed y / x stages
+    ((64, 128, 512), (2, 2, 1), (1, 2, 2)),
+    ((512, 16, 32), (2, 1, 1), (1, 2, 1)),
+])
+def test_compensated_fp32_last_pass(gin, tin, tout):
+    """float32_compensated (last radix pass in hi + lo float pairs with exact
+    twiddle products and two-sum additions) stays within the FP32 bound and is
+    at least as accurate as the plain FP32 form on the same inputs."""
+    x = random_input(gin, False, 5, "float32")
+    ref = O.global_fft(x, (0, 1, 2), False)
+    errs = {}
+    for prec in ("float32", "float32_compensated"):
+        plan = dfft.Plan(gin, gin, (0, 1, 2), tin, tout, precision=prec)
+        X = run(plan, x, True)
+        errs[prec] = O.rel_l2(X, ref)
+        xb = run(plan, ref.astype(np.complex64), False)
+        assert O.rel_l2(xb, O.global_ifft(ref.astype(np.complex64), (0, 1, 2), False, gin)) <= 1e-6
+        assert plan.device_error() == 0
+    assert errs["float32_compensated"] <= 1e-6
+    assert errs["float32_compensated"] <= errs["float32"] * 1.02, errs

@@ -555,6 +555,22 @@ dfft_status dfft_ns_write_diagnostics(dfft_ns* ns, const void* uk, const char* o
   });
 }
 
+dfft_status dfft_ns_rhs_adjoint(dfft_ns* ns, const void* uk, const void* lambda, void* grad, void* stream) {
+  return guarded([&] {
+    if (!uk || !lambda || !grad) dfft::fail(dfft::kErrInvalidArgument, "null buffer");
+    if (grad == uk || grad == lambda) dfft::fail(dfft::kErrInvalidArgument, "grad must not alias uk or lambda");
+    dfft::ns_rhs_adjoint(ns_of(ns), uk, lambda, grad, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_ns_step_adjoint(dfft_ns* ns, const void* uk, void* lambda, void* stream) {
+  return guarded([&] {
+    if (!uk || !lambda) dfft::fail(dfft::kErrInvalidArgument, "null buffer");
+    if (uk == lambda) dfft::fail(dfft::kErrInvalidArgument, "lambda must not alias uk");
+    dfft::ns_step_adjoint(ns_of(ns), uk, lambda, static_cast<cudaStream_t>(stream));
+  });
+}
+
 dfft_status dfft_ns_destroy(dfft_ns* ns) {
   return guarded([&] {
     if (!ns) return;

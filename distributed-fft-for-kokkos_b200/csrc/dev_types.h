@@ -125,7 +125,7 @@ int pair_stage_line_options(int n, bool afast, int* opts);
 int pair_stage_stream_lines(int n, bool afast);
 cudaError_t launch_fft_pair(const StageArgs& A, bool inverse, bool afast, cudaStream_t st);
 // TMA-fed two-line stage (fft_tma.cu): b-fast C2C tiles of 2^k complex64
-// points (16..512) whose source is described by a tiled tensor map `map`
+// points (16..1024) whose source is described by a tiled tensor map `map`
 // (a CUtensorMap, 128 bytes) with boxes of A.B x min(n, 256);
 // A.B must be one of pair_tma_line_options(n) and A.err a device int.
 bool pair_tma_supported(int n);

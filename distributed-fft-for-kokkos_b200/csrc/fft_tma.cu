@@ -391,7 +391,7 @@ cudaError_t launch_tma_n(const StageArgs& A, const void* map, const TmaCoords& T
 
 }  // namespace
 
-bool pair_tma_supported(int n) { return n >= 16 && n <= 512 && (n & (n - 1)) == 0; }
+bool pair_tma_supported(int n) { return n >= 16 && n <= 1024 && (n & (n - 1)) == 0; }
 
 int pair_tma_lines(int n) { return pair_tma_supported(n) ? 2 * pair_stream_pairs(n) : 0; }
 
@@ -411,7 +411,7 @@ cudaError_t launch_fft_pair_tma(const StageArgs& A, const void* map, const TmaCo
   switch (A.n) {
 #define DFFT_TMA(N_) \
   case N_: return inverse ? launch_tma_n<N_, true>(A, map, T, st) : launch_tma_n<N_, false>(A, map, T, st);
-    DFFT_TMA(16) DFFT_TMA(32) DFFT_TMA(64) DFFT_TMA(128) DFFT_TMA(256) DFFT_TMA(512)
+    DFFT_TMA(16) DFFT_TMA(32) DFFT_TMA(64) DFFT_TMA(128) DFFT_TMA(256) DFFT_TMA(512) DFFT_TMA(1024)
 #undef DFFT_TMA
     default: return cudaErrorInvalidValue;
   }

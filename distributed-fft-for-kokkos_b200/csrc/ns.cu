@@ -324,6 +324,140 @@ __global__ void ns_diag_kernel(const DevLayout L, const cplx<T>* uk, NsGeom g, d
     if (ss[i] != 0.0) atomicAdd(out + 3 + i, ss[i]);
 }
 
+// ---- adjoint (vector-Jacobian product) of the right-hand side ----
+// f(y) = P(-D F(adv(B D y)) - nu k^2 D y), adv_j = sum_a u_a d_a u_j, u = B D y,
+// d_a u = B(i k_a D y); D the 2/3 mask, P the projection, F / B the forward /
+// backward transforms.  With the real inner product on the half spectrum
+// (Re sum conj(a) b, as the plan's adjoint transforms use) the VJP of a
+// cotangent c is
+//   mu = P c,   lambda_adv = F^H(-D mu),
+//   lambda_u_a = sum_j lambda_adv_j d_a u_j,   lambda_(d_a u)_j = u_a lambda_adv_j,
+//   f^T c = D(-nu k^2 mu + B^H lambda_u + sum_a (-i k_a) B^H lambda_(d_a u)).
+
+// dst = D src
+template <typename T>
+__global__ void ns_dealias_kernel(const DevLayout L, const cplx<T>* src, cplx<T>* dst, NsGeom g) {
+  const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int iz = static_cast<int>(t % g.nzh);
+    const int iy = static_cast<int>((t / g.nzh) % g.ny);
+    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    const bool keep = abs(signed_mode(ix, g.nx)) <= g.cx && abs(signed_mode(iy, g.ny)) <= g.cy && iz <= g.cz;
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dst[o[d]] = keep ? src[o[d]] : mk<T>(T(0), T(0));
+  }
+}
+
+// mu = P c (projection, 1/k^2 = 0 at the origin); advbar = -D mu
+template <typename T>
+__global__ void ns_adj_pre_kernel(const DevLayout L, const cplx<T>* c, cplx<T>* mu, cplx<T>* advbar, NsGeom g) {
+  const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int iz = static_cast<int>(t % g.nzh);
+    const int iy = static_cast<int>((t / g.nzh) % g.ny);
+    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
+    const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
+    const double kx = mx * g.kscale, ky = my * g.kscale, kz = mz * g.kscale;
+    const double inv_ksq = (ix == 0 && iy == 0 && iz == 0) ? 0.0 : 1.0 / (kx * kx + ky * ky + kz * kz);
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
+    cplx<T> r[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[d] = c[o[d]];
+    const T ikk = T(inv_ksq);
+    const cplx<T> div = mk<T>((T(kx) * r[0].x + T(ky) * r[1].x + T(kz) * r[2].x) * ikk,
+                              (T(kx) * r[0].y + T(ky) * r[1].y + T(kz) * r[2].y) * ikk);
+    const T kk[3] = {T(kx), T(ky), T(kz)};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const cplx<T> m = mk<T>(r[d].x - kk[d] * div.x, r[d].y - kk[d] * div.y);
+      mu[o[d]] = m;
+      advbar[o[d]] = keep ? mk<T>(-m.x, -m.y) : mk<T>(T(0), T(0));
+    }
+  }
+}
+
+// physical space, in place: lam <- lambda_u (sum_j lam_j d_a u_j), du[a] <-
+// lambda_(d_a u) (u_a lam_j)
+template <typename T>
+__global__ void ns_adj_point_kernel(const DevLayout L, const T* u, T* d0, T* d1, T* d2, T* lam, NsGeom g) {
+  const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nz;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int iz = static_cast<int>(t % g.nz);
+    const int iy = static_cast<int>((t / g.nz) % g.ny);
+    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nz) * g.ny));
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
+    T* dd[3] = {d0, d1, d2};
+    T uu[3], la[3], gr[3][3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      uu[j] = u[o[j]];
+      la[j] = lam[o[j]];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) gr[a][j] = dd[a][o[j]];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      lam[o[a]] = la[0] * gr[a][0] + la[1] * gr[a][1] + la[2] * gr[a][2];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) dd[a][o[j]] = uu[a] * la[j];
+    }
+  }
+}
+
+// out = D(-nu k^2 mu + w + sum_a (-i k_a) h_a)
+template <typename T>
+__global__ void ns_adj_combine_kernel(const DevLayout L, const cplx<T>* mu, const cplx<T>* w, const cplx<T>* h0,
+                                      const cplx<T>* h1, const cplx<T>* h2, cplx<T>* out, NsGeom g, double nu) {
+  const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int iz = static_cast<int>(t % g.nzh);
+    const int iy = static_cast<int>((t / g.nzh) % g.ny);
+    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
+    const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
+    const double kx = mx * g.kscale, ky = my * g.kscale, kz = mz * g.kscale;
+    const T visc = T(-nu * (kx * kx + ky * ky + kz * kz));
+    const T kk[3] = {T(kx), T(ky), T(kz)};
+    int64_t o[3];
+    off3(L, ix, iy, iz, o);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int64_t q = o[d];
+      if (!keep) {
+        out[q] = mk<T>(T(0), T(0));
+        continue;
+      }
+      const cplx<T> m = mu[q], ww = w[q], a0 = h0[q], a1 = h1[q], a2 = h2[q];
+      // -i k z = (k z.y, -k z.x)
+      const T sy = kk[0] * a0.y + kk[1] * a1.y + kk[2] * a2.y;
+      const T sx = kk[0] * a0.x + kk[1] * a1.x + kk[2] * a2.x;
+      out[q] = mk<T>(visc * m.x + ww.x + sy, visc * m.y + ww.y - sx);
+    }
+  }
+}
+
+// y = a + s x over whole buffers (n complex elements)
+template <typename T>
+__global__ void ns_axpy_kernel(const cplx<T>* a, const cplx<T>* x, cplx<T>* y, double s, int64_t n) {
+  const T ss = T(s);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const cplx<T> av = a[i], xv = x[i];
+    y[i] = mk<T>(av.x + ss * xv.x, av.y + ss * xv.y);
+  }
+}
+
 unsigned grid_of(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
@@ -349,7 +483,13 @@ struct NsState {
   double* energy = nullptr;
   double* diag = nullptr;  // 3 + kNsMaxBins sums of ns_diagnostics
   double* bins = nullptr;  // kNsMaxBins + 1 bin edges
+  // adjoint workspace (allocated by the first adjoint call): spectral mu, w,
+  // lambda_y0, lambda_k, vjp output; physical lambda_adv
+  void* adj[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  void* ladv = nullptr;
   ~NsState() {
+    for (auto p : adj) cudaFree(p);
+    cudaFree(ladv);
     for (auto p : dk) cudaFree(p);
     for (auto p : du) cudaFree(p);
     for (auto p : rk) cudaFree(p);
@@ -610,6 +750,127 @@ NsDiag ns_write_diagnostics(NsState* s, const void* uk, const std::string& dir, 
   write_raw(dump_name(dir, "E_spec", 0, 0, iter), spec.data(), spec.size() * sizeof(double));
   write_raw(dump_name(dir, "k_vals", 0, 0, iter), kv.data(), kv.size() * sizeof(double));
   return r;
+}
+
+// ---- adjoints ----
+static void ns_adj_alloc(NsState* s) {
+  if (s->ladv) return;
+  const std::size_t cb = (s->dbl ? 16 : 8) * s->nout, rb = (s->dbl ? 8 : 4) * s->nin;
+  for (auto& p : s->adj) ck(cudaMalloc(&p, cb), "ns adjoint alloc");
+  ck(cudaMalloc(&s->ladv, rb), "ns adjoint alloc");
+}
+
+template <typename T>
+static void launch_dealias(NsState* s, const void* src, void* dst, cudaStream_t st) {
+  using namespace dev;
+  const int64_t nsp = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nzh;
+  ns_dealias_kernel<T><<<grid_of(nsp), 256, 0, st>>>(s->lout, static_cast<const cplx<T>*>(src),
+                                                      static_cast<cplx<T>*>(dst), s->g);
+  ck(cudaGetLastError(), "ns dealias");
+}
+
+template <typename T>
+static void launch_axpy(const void* a, const void* x, void* y, double sc, std::size_t n, cudaStream_t st) {
+  using namespace dev;
+  ns_axpy_kernel<T><<<grid_of(static_cast<int64_t>(n)), 256, 0, st>>>(
+      static_cast<const cplx<T>*>(a), static_cast<const cplx<T>*>(x), static_cast<cplx<T>*>(y), sc,
+      static_cast<int64_t>(n));
+  ck(cudaGetLastError(), "ns axpy");
+}
+
+// out = (d f / d y)^T c at y; y is one of the adjoint's own buffers (it is
+// dealiased in place, a no-op for the dealiased states the callers pass).
+template <typename T>
+static void ns_vjp(NsState* s, void* y, const void* c, void* out, cudaStream_t st) {
+  using namespace dev;
+  using C = cplx<T>;
+  const int64_t nsp = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nzh;
+  const int64_t nph = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nz;
+  // recompute u and d_a u from y (the forward pencils are not stored)
+  ns_prep_kernel<T><<<grid_of(nsp), 256, 0, st>>>(s->lout, static_cast<C*>(y), static_cast<C*>(s->dk[0]),
+                                                   static_cast<C*>(s->dk[1]), static_cast<C*>(s->dk[2]), s->g);
+  ck(cudaGetLastError(), "ns vjp prep");
+  s->plan->execute(y, s->u, false, st);
+  for (int k = 0; k < 3; ++k) s->plan->execute(s->dk[k], s->du[k], false, st);
+  void* mu = s->adj[0];
+  void* w = s->adj[1];
+  ns_adj_pre_kernel<T><<<grid_of(nsp), 256, 0, st>>>(s->lout, static_cast<const C*>(c), static_cast<C*>(mu),
+                                                      static_cast<C*>(s->adv), s->g);
+  ck(cudaGetLastError(), "ns vjp projection");
+  s->plan->execute_adjoint(s->adv, s->ladv, true, st);  // F^H
+  ns_adj_point_kernel<T><<<grid_of(nph), 256, 0, st>>>(s->lin, static_cast<const T*>(s->u),
+                                                        static_cast<T*>(s->du[0]), static_cast<T*>(s->du[1]),
+                                                        static_cast<T*>(s->du[2]), static_cast<T*>(s->ladv), s->g);
+  ck(cudaGetLastError(), "ns vjp advection");
+  s->plan->execute_adjoint(s->ladv, w, false, st);  // B^H
+  for (int k = 0; k < 3; ++k) s->plan->execute_adjoint(s->du[k], s->dk[k], false, st);
+  ns_adj_combine_kernel<T><<<grid_of(nsp), 256, 0, st>>>(
+      s->lout, static_cast<const C*>(mu), static_cast<const C*>(w), static_cast<const C*>(s->dk[0]),
+      static_cast<const C*>(s->dk[1]), static_cast<const C*>(s->dk[2]), static_cast<C*>(out), s->g, s->nu);
+  ck(cudaGetLastError(), "ns vjp combine");
+}
+
+template <typename T>
+static void ns_rhs_adjoint_t(NsState* s, const void* uk, const void* lam, void* grad, cudaStream_t st) {
+  ns_adj_alloc(s);
+  void* y = s->rk[0];
+  launch_dealias<T>(s, uk, y, st);
+  ns_vjp<T>(s, y, lam, grad, st);
+}
+
+// One RK4 step S(y) = D y + (k1 + 2 k2 + 2 k3 + k4) / 6, k_i = dt f(a_i),
+// a1 = D y, a2 = a1 + k1 / 2, a3 = a1 + k2 / 2, a4 = a1 + k3: the stage
+// states are recomputed from y (three right-hand sides), then the four VJPs
+// run backwards.
+template <typename T>
+static void ns_step_adjoint_t(NsState* s, const void* uk, void* lam, cudaStream_t st) {
+  ns_adj_alloc(s);
+  const double h = s->dt;
+  const std::size_t n = s->nout;
+  void* a[4] = {s->rk[0], s->rk[1], s->rk[2], s->rk[3]};
+  void* ly0 = s->adj[2];
+  void* lk = s->adj[3];
+  void* gbuf = s->adj[4];
+  launch_dealias<T>(s, uk, a[0], st);
+  for (int i = 1; i < 4; ++i) {
+    // f(a_{i-1}) into gbuf (the right-hand side dealiases its input in place:
+    // the stage states are already dealiased)
+    ns_rhs_stage(s, a[i - 1], -1, gbuf, st);
+    launch_axpy<T>(a[0], gbuf, a[i], i == 3 ? h : 0.5 * h, n, st);
+  }
+  // backward pass: ly0 accumulates the cotangent of a1, lk is the cotangent
+  // of the current k_i
+  ck(cudaMemcpyAsync(ly0, lam, n * sizeof(dev::cplx<T>), cudaMemcpyDeviceToDevice, st), "ns step adjoint");
+  const double ck_direct[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};  // d S / d k_i
+  const double up[3] = {0.5, 0.5, 1.0};  // a2 = a1 + k1 / 2, a3 = a1 + k2 / 2, a4 = a1 + k3
+  // k4 first: lk = lam / 6
+  launch_axpy<T>(lam, lam, lk, ck_direct[3] - 1.0, n, st);
+  for (int i = 3; i >= 0; --i) {
+    // g = dt f'(a_i)^T lk
+    ns_vjp<T>(s, a[i], lk, gbuf, st);
+    launch_axpy<T>(ly0, gbuf, ly0, h, n, st);
+    if (i > 0) {
+      // cotangent of k_i (1-based; a[i] = a1 + up[i - 1] k_i): its direct
+      // weight in S plus up[i - 1] times this stage's g
+      launch_axpy<T>(lam, lam, lk, ck_direct[i - 1] - 1.0, n, st);
+      launch_axpy<T>(lk, gbuf, lk, h * up[i - 1], n, st);
+    }
+  }
+  launch_dealias<T>(s, ly0, lam, st);
+}
+
+void ns_rhs_adjoint(NsState* s, const void* uk, const void* lam, void* grad, cudaStream_t st) {
+  if (s->dbl)
+    ns_rhs_adjoint_t<double>(s, uk, lam, grad, st);
+  else
+    ns_rhs_adjoint_t<float>(s, uk, lam, grad, st);
+}
+
+void ns_step_adjoint(NsState* s, const void* uk, void* lam, cudaStream_t st) {
+  if (s->dbl)
+    ns_step_adjoint_t<double>(s, uk, lam, st);
+  else
+    ns_step_adjoint_t<float>(s, uk, lam, st);
 }
 
 void ns_destroy(NsState* s) { delete s; }

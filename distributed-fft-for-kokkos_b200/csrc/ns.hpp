@@ -26,5 +26,10 @@ void ns_vorticity(NsState* s, const void* uk, void* vor, cudaStream_t st);
 NsDiag ns_diagnostics(NsState* s, const void* uk, int nb, double* spec, double* kvals, cudaStream_t st);
 // the reference's diag_fields + diag_energy files for every virtual rank
 NsDiag ns_write_diagnostics(NsState* s, const void* uk, const std::string& dir, int iter, int nb, cudaStream_t st);
+// VJPs with the real inner product of the half spectrum: grad = (d f / d uk)^T
+// lam for f(uk) = rhs(D uk); lam <- (d S / d uk)^T lam for one RK4 step S
+// (the stage states are recomputed from uk, not stored); uk is not modified
+void ns_rhs_adjoint(NsState* s, const void* uk, const void* lam, void* grad, cudaStream_t st);
+void ns_step_adjoint(NsState* s, const void* uk, void* lam, cudaStream_t st);
 void ns_destroy(NsState* s);
 }  // namespace dfft

@@ -142,6 +142,9 @@ SIGNATURES = {
     "dfft_ns_write_diagnostics": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
                        ctypes.POINTER(NsDiag), ctypes.c_void_p]),
+    "dfft_ns_rhs_adjoint": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_ns_step_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "dfft_ns_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dfft_pack": (
         ctypes.c_int, [ctypes.c_int32, _U64P, _I32P, ctypes.c_int32, _U64P, ctypes.c_int32, ctypes.c_int32,

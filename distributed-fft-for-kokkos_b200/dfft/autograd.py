@@ -6,13 +6,20 @@ plan's adjoint (``dfft_execute_adjoint``) in the backward pass, on the
 concatenated per-rank buffers.  With PyTorch's convention for complex
 gradients the gradient of a real loss with respect to a real R2C input is
 Re(F^H g), which is exactly what the Hermitian-weighted adjoint computes.
+
+``navier_stokes(u0, ns, steps)`` runs the pseudo-spectral solver from a
+physical field u0 (forward transform, ``steps`` RK4 steps, backward
+transform) and back-propagates with the step adjoint
+(``dfft_ns_step_adjoint``), which recomputes each step's stage states from the
+step's input state; only those states are kept (one spectral buffer per
+step).
 """
 import torch
 
 from .plan import Direction, execute, execute_adjoint
 
-_COMPLEX = {"float64": torch.complex128, "float32": torch.complex64}
-_REAL = {"float64": torch.float64, "float32": torch.float32}
+_COMPLEX = {"float64": torch.complex128, "float32": torch.complex64, "float32_compensated": torch.complex64}
+_REAL = {"float64": torch.float64, "float32": torch.float32, "float32_compensated": torch.float32}
 
 
 def _dtypes(plan):
@@ -44,3 +51,41 @@ class DistributedFFTFunction(torch.autograd.Function):
 
 def fft(x, plan, direction=Direction.forward):
     return DistributedFFTFunction.apply(x, plan, direction)
+
+
+class NavierStokesFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, u0, ns, steps):
+        plan = ns._plan
+        din, dout = _dtypes(plan)
+        stream = torch.cuda.current_stream().cuda_stream
+        uk = torch.empty(plan.buffer_elements("out"), dtype=dout, device=u0.device)
+        execute(plan, u0.contiguous(), uk, Direction.forward, stream=stream)
+        states = []
+        for _ in range(int(steps)):
+            states.append(uk.clone())
+            ns.step(uk, stream=stream)
+        uT = torch.empty(plan.buffer_elements("in"), dtype=din, device=u0.device)
+        execute(plan, uk, uT, Direction.backward, stream=stream)
+        ctx.ns, ctx.states = ns, states
+        return uT
+
+    @staticmethod
+    def backward(ctx, g):
+        ns = ctx.ns
+        plan = ns._plan
+        din, dout = _dtypes(plan)
+        stream = torch.cuda.current_stream().cuda_stream
+        lam = torch.empty(plan.buffer_elements("out"), dtype=dout, device=g.device)
+        execute_adjoint(plan, g.contiguous(), lam, Direction.backward, stream=stream)
+        for uk in reversed(ctx.states):
+            ns.step_adjoint(uk, lam, stream=stream)
+        grad = torch.empty(plan.buffer_elements("in"), dtype=din, device=g.device)
+        execute_adjoint(plan, lam, grad, Direction.forward, stream=stream)
+        ctx.states = None
+        return grad, None, None
+
+
+def navier_stokes(u0, ns, steps):
+    """u(T) after `steps` RK4 steps of the solver `ns` from the physical field u0."""
+    return NavierStokesFunction.apply(u0, ns, steps)

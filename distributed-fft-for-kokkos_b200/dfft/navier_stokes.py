@@ -46,6 +46,14 @@ class NavierStokes:
         _check(lib.dfft_ns_energy(self._h, _ptr(uk), ctypes.byref(e), self._stream(stream)))
         return e.value
 
+    def rhs_adjoint(self, uk, lam, grad, stream=None):
+        """grad = (d rhs / d uk)^T lam (real inner product of the half spectrum)."""
+        _check(lib.dfft_ns_rhs_adjoint(self._h, _ptr(uk), _ptr(lam), _ptr(grad), self._stream(stream)))
+
+    def step_adjoint(self, uk, lam, stream=None):
+        """lam <- (d step / d uk)^T lam for one RK4 step from state uk."""
+        _check(lib.dfft_ns_step_adjoint(self._h, _ptr(uk), _ptr(lam), self._stream(stream)))
+
     def velocity(self, uk, u, stream=None):
         _check(lib.dfft_ns_velocity(self._h, _ptr(uk), _ptr(u), self._stream(stream)))
 

@@ -263,6 +263,22 @@ dfft_status dfft_ns_diagnostics(dfft_ns* ns, const void* uk, int32_t num_bins, d
  * Synchronises the stream. */
 dfft_status dfft_ns_write_diagnostics(dfft_ns* ns, const void* uk, const char* out_dir, int32_t iter,
                                       int32_t num_bins, dfft_ns_diag* out, void* stream);
+/* Adjoints of the right-hand side and of the RK4 step, for gradients
+ * through the solver.  Cotangents live in the spectral (output) layout and
+ * pair with tangents through the real inner product Re sum conj(a) b over the
+ * stored half spectrum, the inner product of dfft_execute_adjoint.
+ *   dfft_ns_rhs_adjoint:  grad = (d f / d uk)^T lambda for f(uk) = the
+ *     right-hand side of dfft_ns_rhs at uk (which first dealiases uk); the
+ *     physical velocity and its gradients are recomputed from uk (nine
+ *     transforms), nothing of a forward call is stored;
+ *   dfft_ns_step_adjoint: lambda <- (d S / d uk)^T lambda for one RK4 step S
+ *     of dfft_ns_step from state uk; the four stage states are recomputed from
+ *     uk (three right-hand sides), then the four stage VJPs run backwards.
+ * uk and lambda are not modified (except lambda's update in the step
+ * adjoint).  The first call allocates the adjoint workspace (five spectral
+ * and one physical buffer).  No counterpart in the reference. */
+dfft_status dfft_ns_rhs_adjoint(dfft_ns* ns, const void* uk, const void* lambda, void* grad, void* stream);
+dfft_status dfft_ns_step_adjoint(dfft_ns* ns, const void* uk, void* lambda, void* stream);
 dfft_status dfft_ns_destroy(dfft_ns* ns);
 
 /* get_all_slab_topologies (pencil = 0) / get_all_pencil_topologies (pencil = 1),

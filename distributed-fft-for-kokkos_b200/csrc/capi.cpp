@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/dfft.h"
+#include "batch.hpp"
 #include "exchange.hpp"
 #include "ns.hpp"
 #include "plan.hpp"
@@ -24,6 +25,10 @@ struct dfft_ns_s {
 struct dfft_graph_s {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+};
+
+struct dfft_batch_s {
+  dfft::Batch* impl;
 };
 
 namespace {
@@ -108,6 +113,42 @@ dfft_status create(dfft_plan** out, const dfft_plan_desc* desc, bool on_device) 
 }
 
 }  // namespace
+
+// Capture `body` (work enqueued on one stream) into an instantiated graph.
+template <typename F>
+static dfft_graph_s* capture_graph(F&& body) {
+  auto ck = [](cudaError_t e, const char* what) {
+    if (e != cudaSuccess) dfft::fail(dfft::kErrCuda, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  cudaStream_t cap = nullptr;
+  ck(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream create");
+  cudaGraph_t g = nullptr;
+  try {
+    ck(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      body(cap);
+    } catch (...) {
+      cudaGraph_t dead = nullptr;
+      cudaStreamEndCapture(cap, &dead);
+      if (dead) cudaGraphDestroy(dead);
+      throw;
+    }
+    ck(cudaStreamEndCapture(cap, &g), "end capture");
+  } catch (...) {
+    cudaStreamDestroy(cap);
+    throw;
+  }
+  cudaStreamDestroy(cap);
+  auto* out = new dfft_graph_s;
+  out->graph = g;
+  if (cudaGraphInstantiate(&out->exec, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    delete out;
+    dfft::fail(dfft::kErrCuda, "cudaGraphInstantiate failed");
+  }
+  return out;
+}
 
 extern "C" {
 
@@ -449,6 +490,67 @@ dfft_status dfft_graph_create(dfft_graph** graph, const dfft_plan* const* plans,
       throw;
     }
     cleanup();
+  });
+}
+
+static const dfft::Batch& batch_of(const dfft_batch* b) {
+  if (!b || !b->impl) dfft::fail(dfft::kErrInvalidArgument, "null batch");
+  return *b->impl;
+}
+
+dfft_status dfft_batch_create(dfft_batch** batch, const dfft_plan* const* plans, int64_t count) {
+  return guarded([&] {
+    if (!batch || !plans || count <= 0) dfft::fail(dfft::kErrInvalidArgument, "null argument or empty batch");
+    *batch = nullptr;
+    std::vector<const dfft::Plan*> ps;
+    for (int64_t i = 0; i < count; ++i) ps.push_back(&impl_of(plans[i]));
+    auto* impl = new dfft::Batch(std::move(ps));
+    *batch = new dfft_batch_s{impl};
+  });
+}
+
+dfft_status dfft_batch_execute(const dfft_batch* batch, const void* const* ins, void* const* outs, int32_t direction,
+                               void* stream) {
+  return guarded([&] {
+    if (direction != DFFT_FORWARD && direction != DFFT_BACKWARD)
+      dfft::fail(dfft::kErrInvalidArgument, "Invalid FFT direction specified.");
+    batch_of(batch).execute(ins, outs, direction == DFFT_FORWARD, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_batch_get_launch_count(const dfft_batch* batch, int32_t direction, int64_t* launches) {
+  return guarded([&] {
+    if (!launches) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *launches = static_cast<int64_t>(batch_of(batch).launches(direction == DFFT_FORWARD));
+  });
+}
+
+dfft_status dfft_batch_destroy(dfft_batch* batch) {
+  return guarded([&] {
+    if (!batch) return;
+    delete batch->impl;
+    delete batch;
+  });
+}
+
+dfft_status dfft_ns_graph_create(dfft_graph** graph, dfft_ns* const* states, void* const* uks, int64_t count) {
+  return guarded([&] {
+    if (!graph || !states || !uks || count <= 0) dfft::fail(dfft::kErrInvalidArgument, "null argument or empty batch");
+    *graph = nullptr;
+    std::vector<dfft::NsState*> ss;
+    std::vector<const dfft::Plan*> ps;
+    for (int64_t i = 0; i < count; ++i) {
+      if (!states[i] || !states[i]->impl || !uks[i]) dfft::fail(dfft::kErrInvalidArgument, "null state or buffer");
+      ss.push_back(states[i]->impl);
+      ps.push_back(dfft::ns_plan(states[i]->impl));
+    }
+    for (int64_t i = 0; i < count; ++i)
+      for (int64_t j = 0; j < i; ++j)
+        if (ss[i] == ss[j]) dfft::fail(dfft::kErrInvalidArgument, "a Navier-Stokes state appears twice");
+    const dfft::Batch batch(ps);
+    *graph = capture_graph([&](cudaStream_t st) {
+      dfft::ns_batch_step(ss.data(), uks, static_cast<int>(count), batch, st);
+    });
   });
 }
 

@@ -134,6 +134,22 @@ int pair_tma_lines(int n);
 int pair_tma_line_options(int n, int* opts);
 cudaError_t launch_fft_pair_tma(const StageArgs& A, const void* map, const TmaCoords& T, bool inverse,
                                 cudaStream_t st);
+// Batched register stage (fft_batch.cu): one persistent launch runs the same
+// stage (kind, direction, row orientation) of up to kMaxBatchFields fields of
+// any supported line lengths; field f owns work items prefix[f] .. prefix[f+1]
+// - 1, its tiles (tb + tiles_b (co0 + Eo0 co1)).  Every field's StageArgs
+// must have B = batch_stage_lines(n) (complex lines per tile) and the tiles_b
+// that goes with it; the args are taken by value (kernel parameter space).
+constexpr int kMaxBatchFields = 48;
+struct BatchParams {
+  int nfields;
+  long long prefix[kMaxBatchFields + 1];
+  StageArgs f[kMaxBatchFields];
+};
+bool batch_stage_supported(int n);
+int batch_stage_lines(int n);
+// kind: kC2C, kR2C or kC2R (R2C / C2R: lines along a on both sides)
+cudaError_t launch_fft_batch(BatchParams& P, bool dbl, int kind, bool inverse, bool afast, cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
 cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);

@@ -21,6 +21,7 @@
 
 #include "../../include/dfft.h"
 #include "fft_stage.cuh"
+#include "batch.hpp"
 #include "layout.hpp"
 #include "ns.hpp"
 #include "plan.hpp"
@@ -551,10 +552,13 @@ NsState* ns_create(const Plan* plan, double nu, double dt, double lx) {
 }
 
 // step in 0..3: RK4 stage; step = -1: only the right-hand side, into `out`
-static void ns_rhs_stage(NsState* s, void* uk, int step, void* out, cudaStream_t st) {
+// The three pointwise phases of one right-hand side, around the transforms:
+// prep (dealias uk in place, i k uk), advection (u . grad u in physical
+// space), combine (dealias, -adv - nu k^2 uk, projection, RK4 stage `step`;
+// step = -1 stores the right-hand side into `adv`).
+static void ns_prep_phase(NsState* s, void* uk, cudaStream_t st) {
   using namespace dev;
   const int64_t nsp = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nzh;
-  const int64_t nph = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nz;
   if (s->dbl)
     ns_prep_kernel<double><<<grid_of(nsp), 256, 0, st>>>(s->lout, static_cast<double2*>(uk),
                                                           static_cast<double2*>(s->dk[0]),
@@ -566,8 +570,11 @@ static void ns_rhs_stage(NsState* s, void* uk, int step, void* out, cudaStream_t
                                                          static_cast<float2*>(s->dk[1]),
                                                          static_cast<float2*>(s->dk[2]), s->g);
   ck(cudaGetLastError(), "ns prep");
-  s->plan->execute(uk, s->u, false, st);
-  for (int k = 0; k < 3; ++k) s->plan->execute(s->dk[k], s->du[k], false, st);
+}
+
+static void ns_advection_phase(NsState* s, cudaStream_t st) {
+  using namespace dev;
+  const int64_t nph = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nz;
   if (s->dbl)
     ns_advection_kernel<double><<<grid_of(nph), 256, 0, st>>>(s->lin, static_cast<double*>(s->u),
                                                                static_cast<double*>(s->du[0]),
@@ -579,8 +586,11 @@ static void ns_rhs_stage(NsState* s, void* uk, int step, void* out, cudaStream_t
                                                               static_cast<float*>(s->du[1]),
                                                               static_cast<float*>(s->du[2]), s->g);
   ck(cudaGetLastError(), "ns advection");
-  void* adv = step < 0 ? out : s->adv;
-  s->plan->execute(s->u, adv, true, st);
+}
+
+static void ns_combine_phase(NsState* s, void* uk, void* adv, int step, cudaStream_t st) {
+  using namespace dev;
+  const int64_t nsp = static_cast<int64_t>(s->g.nx) * s->g.ny * s->g.nzh;
   if (s->dbl)
     ns_rhs_rk_kernel<double><<<grid_of(nsp), 256, 0, st>>>(
         s->lout, static_cast<double2*>(adv), static_cast<double2*>(uk), static_cast<double2*>(s->rk[0]),
@@ -593,6 +603,49 @@ static void ns_rhs_stage(NsState* s, void* uk, int step, void* out, cudaStream_t
         s->dt, step);
   ck(cudaGetLastError(), "ns rhs");
 }
+
+// step in 0..3: RK4 stage; step = -1: only the right-hand side, into `out`
+static void ns_rhs_stage(NsState* s, void* uk, int step, void* out, cudaStream_t st) {
+  ns_prep_phase(s, uk, st);
+  s->plan->execute(uk, s->u, false, st);
+  for (int k = 0; k < 3; ++k) s->plan->execute(s->dk[k], s->du[k], false, st);
+  ns_advection_phase(s, st);
+  void* adv = step < 0 ? out : s->adv;
+  s->plan->execute(s->u, adv, true, st);
+  ns_combine_phase(s, uk, adv, step, st);
+}
+
+// One RK4 step of several fields: the pointwise phases per field, each
+// transform of all fields through one batched execution (one launch per
+// stage).
+void ns_batch_step(NsState* const* s, void* const* uks, int n, const Batch& batch, cudaStream_t st) {
+  std::vector<const void*> ins(n);
+  std::vector<void*> outs(n);
+  for (int step = 0; step < 4; ++step) {
+    for (int f = 0; f < n; ++f) ns_prep_phase(s[f], uks[f], st);
+    for (int f = 0; f < n; ++f) {
+      ins[f] = uks[f];
+      outs[f] = s[f]->u;
+    }
+    batch.execute(ins.data(), outs.data(), false, st);
+    for (int k = 0; k < 3; ++k) {
+      for (int f = 0; f < n; ++f) {
+        ins[f] = s[f]->dk[k];
+        outs[f] = s[f]->du[k];
+      }
+      batch.execute(ins.data(), outs.data(), false, st);
+    }
+    for (int f = 0; f < n; ++f) ns_advection_phase(s[f], st);
+    for (int f = 0; f < n; ++f) {
+      ins[f] = s[f]->u;
+      outs[f] = s[f]->adv;
+    }
+    batch.execute(ins.data(), outs.data(), true, st);
+    for (int f = 0; f < n; ++f) ns_combine_phase(s[f], uks[f], s[f]->adv, step, st);
+  }
+}
+
+const Plan* ns_plan(const NsState* s) { return s->plan; }
 
 void ns_rhs(NsState* s, void* uk, void* dukdt, cudaStream_t st) { ns_rhs_stage(s, uk, -1, dukdt, st); }
 

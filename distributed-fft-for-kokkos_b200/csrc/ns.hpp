@@ -32,4 +32,9 @@ NsDiag ns_write_diagnostics(NsState* s, const void* uk, const std::string& dir, 
 void ns_rhs_adjoint(NsState* s, const void* uk, const void* lam, void* grad, cudaStream_t st);
 void ns_step_adjoint(NsState* s, const void* uk, void* lam, cudaStream_t st);
 void ns_destroy(NsState* s);
+class Batch;
+// one RK4 step of n fields (distinct states), the transforms of all fields
+// batched through `batch`, whose plans are the states' plans in order
+void ns_batch_step(NsState* const* s, void* const* uks, int n, const Batch& batch, cudaStream_t st);
+const Plan* ns_plan(const NsState* s);
 }  // namespace dfft

@@ -1198,10 +1198,17 @@ void Plan::check_alignment(const void* p, bool complex, const char* which) const
                                   std::to_string(align) + " bytes)");
 }
 
-void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream) const {
+void Plan::check_buffers(const void* in, const void* out, bool forward) const {
+  if (!on_device_) fail(kErrInvalidArgument, "plan was created by dfft_plan_analyze and cannot execute");
+  if (!in || !out) fail(kErrInvalidArgument, "null buffer");
+  if (in == out) fail(kErrInvalidArgument, "in-place execution is not supported: in and out must differ");
   // forward: input layout -> complex output layout; backward: the reverse
   check_alignment(in, forward ? lin_.complex : true, "input");
   check_alignment(out, forward ? true : lin_.complex, "output");
+}
+
+void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream) const {
+  check_buffers(in, out, forward);
   run_program(prog_[forward ? 0 : 1], in, out, stream);
 }
 

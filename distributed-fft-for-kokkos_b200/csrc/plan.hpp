@@ -106,6 +106,14 @@ class Plan {
   bool on_device() const { return on_device_; }
   // Device error word (0 or the code a kernel's bounded wait left); reset clears it.
   int device_error(bool reset) const;
+  // Batched execution (batch.cpp): the fused program of a direction, the
+  // plan's device buffers by id, one op's launch, and the checks of execute.
+  const std::vector<Op>& program(bool forward) const { return prog_[forward ? 0 : 1]; }
+  void* device_buffer(int id) const { return bufs_.at(id); }
+  cudaError_t launch_op(const Op& op, const dev::StageArgs& A, cudaStream_t stream) const {
+    return launch_stage(op, A, stream);
+  }
+  void check_buffers(const void* in, const void* out, bool forward) const;
   // Device tables of the caller-facing input / output layouts.
   dev::DevLayout device_layout(bool output) const;
   // Copy a buffer recorded by a capturing literal execution of transpose

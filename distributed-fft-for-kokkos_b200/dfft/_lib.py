@@ -125,6 +125,15 @@ SIGNATURES = {
                        ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
                        ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.c_int64]),
     "dfft_graph_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), ctypes.c_int64]),
+    "dfft_batch_execute": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32,
+                       ctypes.c_void_p]),
+    "dfft_batch_get_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dfft_ns_graph_create": (
+        ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                       ctypes.c_int64]),
     "dfft_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dfft_ns_create": (
         ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_double, ctypes.c_double,

@@ -9,7 +9,7 @@ out_topology (1, 1, px, py) (main.cpp:96-102).
 import ctypes
 
 from ._lib import NS_MAX_BINS, NsDiag, lib
-from .plan import _check, _ptr
+from .plan import Graph, _check, _ptr
 
 
 class NavierStokes:
@@ -84,3 +84,17 @@ class NavierStokes:
         if h is not None and h.value:
             lib.dfft_ns_destroy(h)
             self._h = None
+
+
+def step_graph(states, uks):
+    """A library-owned CUDA graph of one RK4 step of every field (states[i]
+    advances uks[i]), each transform of all fields batched into one launch per
+    stage; ``launch(stream)`` advances all fields by one step."""
+    n = len(states)
+    if len(uks) != n or n == 0:
+        raise ValueError("one spectral buffer per state")
+    st = (ctypes.c_void_p * n)(*[s._h.value for s in states])
+    bufs = (ctypes.c_void_p * n)(*[_ptr(u).value for u in uks])
+    h = ctypes.c_void_p()
+    _check(lib.dfft_ns_graph_create(ctypes.byref(h), st, bufs, n))
+    return Graph._from_handle(h, list(states) + [s._plan for s in states])

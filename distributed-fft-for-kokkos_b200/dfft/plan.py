@@ -284,6 +284,12 @@ class Graph:
         self._h = ctypes.c_void_p()
         _check(lib.dfft_graph_create(ctypes.byref(self._h), plans, ins, outs, dirs, br, n))
 
+    @classmethod
+    def _from_handle(cls, h, keep):
+        g = cls.__new__(cls)
+        g._h, g._keep = h, keep
+        return g
+
     def launch(self, stream=None):
         _check(lib.dfft_graph_launch(self._h, ctypes.c_void_p(int(stream)) if stream else None))
 
@@ -291,6 +297,39 @@ class Graph:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             lib.dfft_graph_destroy(h)
+            self._h = None
+
+
+class Batch:
+    """Batched execution of distinct plans (fields of uneven sizes): one
+    persistent launch per stage of all fields.  ``execute(ins, outs,
+    direction)`` transforms ins[i] -> outs[i] with plans[i]."""
+
+    def __init__(self, plans):
+        n = len(plans)
+        arr = (ctypes.c_void_p * n)(*[p._h.value for p in plans])
+        self._keep = list(plans)  # plans must outlive the batch
+        self._h = ctypes.c_void_p()
+        _check(lib.dfft_batch_create(ctypes.byref(self._h), arr, n))
+
+    def execute(self, ins, outs, direction, stream=None):
+        n = len(self._keep)
+        if len(ins) != n or len(outs) != n:
+            raise DistributedFFTError(Status.INVALID_ARGUMENT, "one input and one output per plan")
+        a = (ctypes.c_void_p * n)(*[_ptr(x).value for x in ins])
+        b = (ctypes.c_void_p * n)(*[_ptr(x).value for x in outs])
+        _check(lib.dfft_batch_execute(self._h, a, b, int(Direction(direction)),
+                                      ctypes.c_void_p(int(stream)) if stream else None))
+
+    def launch_count(self, direction=Direction.forward):
+        n = ctypes.c_int64()
+        _check(lib.dfft_batch_get_launch_count(self._h, int(Direction(direction)), ctypes.byref(n)))
+        return n.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dfft_batch_destroy(h)
             self._h = None
 
 

@@ -207,6 +207,27 @@ dfft_status dfft_graph_create(dfft_graph** graph, const dfft_plan* const* plans,
 dfft_status dfft_graph_launch(const dfft_graph* graph, void* stream);
 dfft_status dfft_graph_destroy(dfft_graph* graph);
 
+/* ---- Batched execution of many plans (fields of uneven sizes) ----
+ * A batch holds distinct, executable fused plans of one precision (the same
+ * plan twice is rejected: its scratch arrays would be shared).  One execute
+ * transforms ins[i] -> outs[i] with plans[i] for every field, in the given
+ * direction, on one stream: each stage index of the fields' programs runs as
+ * one persistent launch per group of stages of the same kind, direction and
+ * row orientation (a work table of every field's tiles, any supported line
+ * lengths: 2^k up to 2048 and 3 * 2^k up to 768, register kernels), instead
+ * of one launch per field; stages outside that set launch per field.  Buffers
+ * follow dfft_execute.  Capture dfft_batch_execute in a CUDA graph to replay
+ * it.  No counterpart in the reference (its batched Navier-Stokes example
+ * drives one plan over 4D views per field,
+ * examples/navier-stokes-MPI-batched/main.cpp:465-468). */
+typedef struct dfft_batch_s dfft_batch;
+dfft_status dfft_batch_create(dfft_batch** batch, const dfft_plan* const* plans, int64_t count);
+dfft_status dfft_batch_execute(const dfft_batch* batch, const void* const* ins, void* const* outs, int32_t direction,
+                               void* stream);
+/* kernel launches of one dfft_batch_execute in a direction */
+dfft_status dfft_batch_get_launch_count(const dfft_batch* batch, int32_t direction, int64_t* launches);
+dfft_status dfft_batch_destroy(dfft_batch* batch);
+
 /* ---- Pseudo-spectral Navier-Stokes step of the reference's batched example
  * (examples/navier-stokes-MPI-batched/main.cpp:518-669, RK4 of
  * examples/utils/math_utils.hpp:90-141) on a plan's buffers.  The plan must be
@@ -226,6 +247,14 @@ dfft_status dfft_ns_step(dfft_ns* ns, void* uk, void* stream);
 /* total kinetic energy of main.cpp:746-766, (lx pi)^3 / N^2 * sum 0.5 factor |uk|^2
  * (factor 1 on kz = 0, else 2), FP64 reduction; synchronises the stream */
 dfft_status dfft_ns_energy(dfft_ns* ns, const void* uk, double* energy, void* stream);
+/* One RK4 time step of `count` fields (distinct states, uks[i] the spectral
+ * buffer of states[i]) captured once into a library-owned CUDA graph: per RK
+ * stage the pointwise phases per field and every transform of all fields
+ * through one batched execution (one launch per stage of the transform).
+ * dfft_graph_launch advances every field by one step; dfft_graph_destroy
+ * frees it.  States and plans must outlive the graph.  No counterpart in the
+ * reference (main.cpp:518-586 loops over the fields' RK4 stages). */
+dfft_status dfft_ns_graph_create(dfft_graph** graph, dfft_ns* const* states, void* const* uks, int64_t count);
 /* Physical velocity of a spectrum (the backward transform of diag_fields,
  * main.cpp:711-724) into a buffer of the plan's input layout; uk is not
  * modified. */

@@ -459,15 +459,7 @@ def main():
         for pl, x, y, z in batch["float64"]:
             dfft.execute(pl, x, y, dfft.Direction.forward)
             dfft.execute(pl, y, z, dfft.Direction.backward)
-    for _ in range(args.warmup):
-        loop64()
-    barrier()
-    e0.record(stream)
-    for _ in range(bsteps):
-        loop64()
-    e1.record(stream)
-    barrier()
-    ms_batch64 = max_over_ranks(e0.elapsed_time(e1) / bsteps)
+    ms_batch64 = timed_launch(loop64)
     batch_bytes = sum(algo_bytes(int(e), 8) for e in edges)
     del batch, bgraph, items, batch_graph, fb, xs, ys, zs
     torch.cuda.empty_cache()
@@ -493,19 +485,23 @@ def main():
     # one RK4 step of all 16 fields in a library-owned CUDA graph: every
     # transform of all fields batched into one launch per stage
     # (dfft_ns_graph_create)
-    ns_graph = dfft.step_graph([f[1] for f in ns_fields["float32"]], [f[2] for f in ns_fields["float32"]])
     ns_steps = max(3, args.steps // 20)
-    for _ in range(args.warmup):
-        ns_graph.launch(stream.cuda_stream)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(ns_steps):
-        ns_graph.launch(stream.cuda_stream)
-    e1.record(stream)
-    barrier()
-    ms_ns32 = max_over_ranks(e0.elapsed_time(e1) / ns_steps)
-    n32 = args.warmup + ns_steps  # RK4 steps the FP32 fields took
+    ms_ns = {}
+    for batched in (True, False):
+        ns_graph = dfft.step_graph([f[1] for f in ns_fields["float32"]], [f[2] for f in ns_fields["float32"]],
+                                   batched=batched)
+        for _ in range(args.warmup):
+            ns_graph.launch(stream.cuda_stream)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ns_steps):
+            ns_graph.launch(stream.cuda_stream)
+        e1.record(stream)
+        barrier()
+        ms_ns[batched] = max_over_ranks(e0.elapsed_time(e1) / ns_steps)
+    ms_ns32 = min(ms_ns.values())
+    n32 = 2 * (args.warmup + ns_steps)  # RK4 steps the FP32 fields took
 
     def ns_loop64():
         for pl, st, uk in ns_fields["float64"]:
@@ -525,7 +521,10 @@ def main():
     e_rel = max(abs(f32[1].energy(f32[2], stream=stream.cuda_stream) / f64[1].energy(f64[2], stream=stream.cuda_stream)
                     - 1.0) for f32, f64 in zip(ns_fields["float32"], ns_fields["float64"]))
     ns_res = {"edges": [int(e) for e in edges], "topology_in": [1, 2, 2, 1], "topology_out": [1, 1, 2, 2],
-              "re": 1600, "dt": 1e-3, "rk4_steps_timed": ns_steps, "fp32_batched_step_graph_ms_per_step": round(ms_ns32, 4),
+              "re": 1600, "dt": 1e-3, "rk4_steps_timed": ns_steps,
+              "fp32_step_graph_ms_per_step": round(ms_ns32, 4),
+              "fp32_batched_transforms_graph_ms": round(ms_ns[True], 4),
+              "fp32_per_field_branches_graph_ms": round(ms_ns[False], 4),
               "fp64_loop_ms_per_step": round(ms_ns64, 4), "speedup": round(ms_ns64 / ms_ns32, 3),
               "transforms_per_step": 20 * len(edges),
               "max_rel_energy_diff_fp32_vs_fp64": e_rel, "sim_time": round(n32 * 1e-3, 4)}

@@ -101,6 +101,7 @@ void Batch::execute(const void* const* ins, void* const* outs, bool forward, cud
         for (int i = 0; i < P.nfields; ++i) {
           P.f[i] = list[c + i];
           const long long tiles = static_cast<long long>(P.f[i].tiles_b) * P.f[i].Eo0 * P.f[i].Eo1;
+          if (tiles >= (1ll << 31)) fail(kErrUnsupported, "too many tiles in one field of a batch");
           P.prefix[i + 1] = P.prefix[i] + tiles;
         }
         const cudaError_t e = dev::launch_fft_batch(P, dbl_, std::get<0>(g.first), std::get<1>(g.first),

@@ -533,7 +533,8 @@ dfft_status dfft_batch_destroy(dfft_batch* batch) {
   });
 }
 
-dfft_status dfft_ns_graph_create(dfft_graph** graph, dfft_ns* const* states, void* const* uks, int64_t count) {
+dfft_status dfft_ns_graph_create(dfft_graph** graph, dfft_ns* const* states, void* const* uks, int64_t count,
+                                 int32_t batched) {
   return guarded([&] {
     if (!graph || !states || !uks || count <= 0) dfft::fail(dfft::kErrInvalidArgument, "null argument or empty batch");
     *graph = nullptr;
@@ -547,10 +548,61 @@ dfft_status dfft_ns_graph_create(dfft_graph** graph, dfft_ns* const* states, voi
     for (int64_t i = 0; i < count; ++i)
       for (int64_t j = 0; j < i; ++j)
         if (ss[i] == ss[j]) dfft::fail(dfft::kErrInvalidArgument, "a Navier-Stokes state appears twice");
-    const dfft::Batch batch(ps);
-    *graph = capture_graph([&](cudaStream_t st) {
-      dfft::ns_batch_step(ss.data(), uks, static_cast<int>(count), batch, st);
-    });
+    if (batched) {
+      const dfft::Batch batch(ps);
+      *graph = capture_graph([&](cudaStream_t st) {
+        dfft::ns_batch_step(ss.data(), uks, static_cast<int>(count), batch, st);
+      });
+      return;
+    }
+    // per-field steps on up to four concurrent branches; fields that share a
+    // plan (and so its scratch) stay on one branch
+    auto ck = [](cudaError_t e, const char* what) {
+      if (e != cudaSuccess) dfft::fail(dfft::kErrCuda, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    std::vector<const dfft::Plan*> distinct;
+    std::vector<int> branch(static_cast<std::size_t>(count));
+    for (int64_t i = 0; i < count; ++i) {
+      auto it = std::find(distinct.begin(), distinct.end(), ps[i]);
+      if (it == distinct.end()) {
+        branch[i] = static_cast<int>(distinct.size());
+        distinct.push_back(ps[i]);
+      } else {
+        branch[i] = static_cast<int>(it - distinct.begin());
+      }
+    }
+    const int nb = static_cast<int>(std::min<std::size_t>(4, distinct.size()));
+    for (auto& b : branch) b %= nb;
+    std::vector<cudaStream_t> streams(nb, nullptr);
+    std::vector<cudaEvent_t> done(nb, nullptr);
+    cudaEvent_t fork = nullptr;
+    auto cleanup = [&]() {
+      for (auto x : streams)
+        if (x) cudaStreamDestroy(x);
+      for (auto e : done)
+        if (e) cudaEventDestroy(e);
+      if (fork) cudaEventDestroy(fork);
+    };
+    try {
+      ck(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event create");
+      for (int b = 0; b < nb; ++b) {
+        ck(cudaStreamCreateWithFlags(&streams[b], cudaStreamNonBlocking), "stream create");
+        ck(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming), "event create");
+      }
+      *graph = capture_graph([&](cudaStream_t st) {
+        ck(cudaEventRecord(fork, st), "fork record");
+        for (int b = 0; b < nb; ++b) ck(cudaStreamWaitEvent(streams[b], fork, 0), "fork wait");
+        for (int64_t i = 0; i < count; ++i) dfft::ns_step(ss[i], uks[i], streams[branch[i]]);
+        for (int b = 0; b < nb; ++b) {
+          ck(cudaEventRecord(done[b], streams[b]), "join record");
+          ck(cudaStreamWaitEvent(st, done[b], 0), "join wait");
+        }
+      });
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
   });
 }
 

@@ -1,0 +1,155 @@
+// Kernels of the batched register stages (see fft_batch.cu): the tile bodies
+// of fft_tile.cuh behind a persistent work-table loop.  Instantiated for
+// general-layout sides (AFF, fft_batch.cu) and separable sides only
+// (fft_batch_sep.cu, fewer registers) in two translation units.
+#pragma once
+
+#include <cstring>
+
+#include "fft_tile.cuh"
+
+namespace dfft {
+namespace dev {
+namespace batch {
+
+using namespace radix;
+
+
+constexpr int kBatchThreads = 256;
+
+// resident CTAs per SM the register budget is sized for: two for complex64
+// (128 registers: every tile body of the switch fits without spills; three,
+// at 80 registers, spilled 100-240 bytes), one for complex128
+template <typename T>
+struct BatchMinBlocks {
+  static constexpr int value = sizeof(T) == 4 ? 2 : 1;
+};
+
+template <int N>
+struct BatchLines {
+  static constexpr int value = kBatchThreads / (N / Vals<N>::value);
+};
+
+#define DFFT_BATCH_LENGTHS(X) \
+  X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(24) X(48) X(96) X(192) X(384) X(768)
+
+// tile (tb, co0, co1) of a field's stage from its local work index (32-bit:
+// the host keeps every field's tile count below 2^31)
+__device__ __forceinline__ void decode(const StageArgs& A, unsigned local, int* tb, int* co0, int* co1) {
+  const unsigned tbs = static_cast<unsigned>(A.tiles_b);
+  *tb = static_cast<int>(local % tbs);
+  const unsigned rest = local / tbs;
+  *co0 = static_cast<int>(rest % static_cast<unsigned>(A.Eo0));
+  *co1 = static_cast<int>(rest / static_cast<unsigned>(A.Eo0));
+}
+
+template <typename T, bool INV, bool AFAST, bool AFF>
+__global__ void __launch_bounds__(kBatchThreads, BatchMinBlocks<T>::value) fft_batch_c2c_kernel(const __grid_constant__ BatchParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long long total = P.prefix[P.nfields];
+  int f = 0, cur_n = 0;
+  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
+    while (w >= P.prefix[f + 1]) ++f;
+    const StageArgs& A = P.f[f];
+    int tb, co0, co1;
+    decode(A, static_cast<unsigned>(w - P.prefix[f]), &tb, &co0, &co1);
+    const bool stage_tw = A.n != cur_n;
+    cur_n = A.n;
+    switch (A.n) {
+#define DFFT_TILE(N_) \
+  case N_: fast_tile<T, INV, N_, BatchLines<N_>::value, AFAST, AFF>(A, tb, co0, co1, smem_raw, stage_tw); break;
+      DFFT_BATCH_LENGTHS(DFFT_TILE)
+#undef DFFT_TILE
+      default: break;
+    }
+    __syncthreads();  // the next tile restages twiddles and lines
+  }
+}
+
+template <typename T, bool C2R, bool AFF>
+__global__ void __launch_bounds__(kBatchThreads, BatchMinBlocks<T>::value) fft_batch_real_kernel(const __grid_constant__ BatchParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long long total = P.prefix[P.nfields];
+  int f = 0, cur_n = 0;
+  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
+    while (w >= P.prefix[f + 1]) ++f;
+    const StageArgs& A = P.f[f];
+    int tb, co0, co1;
+    decode(A, static_cast<unsigned>(w - P.prefix[f]), &tb, &co0, &co1);
+    const bool stage_tw = A.n != cur_n;
+    cur_n = A.n;
+    switch (A.n) {
+#define DFFT_TILE(N_) \
+  case N_: real_tile<T, C2R, N_, BatchLines<N_>::value, AFF>(A, tb, co0, co1, smem_raw, stage_tw); break;
+      DFFT_BATCH_LENGTHS(DFFT_TILE)
+#undef DFFT_TILE
+      default: break;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+size_t tile_smem(int n, bool afast) {
+  switch (n) {
+#define DFFT_SMEM(N_)                                                                                        \
+  case N_:                                                                                                   \
+    return sizeof(cplx<T>) * (N_ + static_cast<size_t>(BatchLines<N_>::value) *                              \
+                                       (afast ? SmemShape<T, N_, BatchLines<N_>::value, true>::LP         \
+                                              : SmemShape<T, N_, BatchLines<N_>::value, false>::LP));
+    DFFT_BATCH_LENGTHS(DFFT_SMEM)
+#undef DFFT_SMEM
+    default: return 0;
+  }
+}
+
+template <typename K>
+cudaError_t launch_persistent(K kernel, BatchParams& P, size_t smem, cudaStream_t st) {
+  cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kernel), smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per_sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBatchThreads, smem)) != cudaSuccess)
+    return e;
+  long long grid = static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1);
+  const long long total = P.prefix[P.nfields];
+  if (grid > total) grid = total;
+  if (grid < 1) return cudaSuccess;
+  kernel<<<static_cast<unsigned>(grid), kBatchThreads, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+template <typename T, bool AFF>
+cudaError_t launch_batch_t(BatchParams& P, int kind, bool inverse, bool afast, cudaStream_t st) {
+  size_t smem = 0;
+  for (int i = 0; i < P.nfields; ++i) {
+    const size_t b = tile_smem<T>(P.f[i].n, kind == kC2C ? afast : true);
+    if (b == 0) return cudaErrorInvalidValue;
+    if (b > smem) smem = b;
+    P.f[i] = with_table_offsets(P.f[i]);
+  }
+  if (kind == kC2C) {
+    if (inverse)
+      return afast ? launch_persistent(fft_batch_c2c_kernel<T, true, true, AFF>, P, smem, st)
+                   : launch_persistent(fft_batch_c2c_kernel<T, true, false, AFF>, P, smem, st);
+    return afast ? launch_persistent(fft_batch_c2c_kernel<T, false, true, AFF>, P, smem, st)
+                 : launch_persistent(fft_batch_c2c_kernel<T, false, false, AFF>, P, smem, st);
+  }
+  if (kind == kR2C) return launch_persistent(fft_batch_real_kernel<T, false, AFF>, P, smem, st);
+  if (kind == kC2R) return launch_persistent(fft_batch_real_kernel<T, true, AFF>, P, smem, st);
+  return cudaErrorInvalidValue;
+}
+
+// the launcher of one addressing variant (AFF: general-layout sides),
+// defined in fft_batch.cu (AFF = true) and fft_batch_sep.cu (AFF = false)
+template <bool AFF>
+cudaError_t launch_batch_variant(BatchParams& P, bool dbl, int kind, bool inverse, bool afast, cudaStream_t st);
+template <>
+cudaError_t launch_batch_variant<true>(BatchParams& P, bool dbl, int kind, bool inverse, bool afast, cudaStream_t st);
+template <>
+cudaError_t launch_batch_variant<false>(BatchParams& P, bool dbl, int kind, bool inverse, bool afast, cudaStream_t st);
+
+}  // namespace batch
+}  // namespace dev
+}  // namespace dfft

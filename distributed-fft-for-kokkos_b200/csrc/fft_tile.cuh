@@ -15,7 +15,10 @@ namespace radix {
 // Called by fft_fast_kernel (one tile per CTA) and by the batched stage
 // kernels (fft_batch.cu), whose CTAs walk tiles of several fields.
 template <typename T, bool INV, int N, int B, bool AFAST, bool AFF>
-__device__ __forceinline__ void fast_tile(const StageArgs& A, int tb, int co0, int co1, unsigned char* smem_raw) {
+// stage_tw = false: the twiddles of this N are already in smem_raw (the
+// previous tile of the CTA had the same line length)
+__device__ __forceinline__ void fast_tile(const StageArgs& A, int tb, int co0, int co1, unsigned char* smem_raw,
+                                          bool stage_tw = true) {
   using C = cplx<T>;
   constexpr int V = Vals<N>::value;
   constexpr int TT = N / V;                  // threads per line
@@ -42,7 +45,8 @@ __device__ __forceinline__ void fast_tile(const StageArgs& A, int tb, int co0, i
 
   {
     const C* gtw = reinterpret_cast<const C*>(A.tw);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+    if (stage_tw)
+      for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   }
 
   // offsets shared by the whole tile (separable tables)
@@ -171,7 +175,8 @@ __device__ __forceinline__ void fast_tile(const StageArgs& A, int tb, int co0, i
 //        assembled in shared memory (imaginary parts of DC and Nyquist
 //        dropped), inverse FFT, x0 = Re z and x1 = Im z are written.
 template <typename T, bool C2R, int N, int B, bool AFF>
-__device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, int co1, unsigned char* smem_raw) {
+__device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, int co1, unsigned char* smem_raw,
+                                          bool stage_tw = true) {
   using C = cplx<T>;
   constexpr int V = Vals<N>::value;
   constexpr int TT = N / V;
@@ -194,7 +199,8 @@ __device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, i
 
   {
     const C* gtw = reinterpret_cast<const C*>(A.tw);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+    if (stage_tw)
+      for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   }
   // row bases (offset of position 0 of each real / complex line); lines are
   // contiguous along a on both sides

@@ -133,7 +133,7 @@ SIGNATURES = {
     "dfft_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dfft_ns_graph_create": (
         ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
-                       ctypes.c_int64]),
+                       ctypes.c_int64, ctypes.c_int32]),
     "dfft_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dfft_ns_create": (
         ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_double, ctypes.c_double,

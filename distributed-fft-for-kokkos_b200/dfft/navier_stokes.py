@@ -86,15 +86,16 @@ class NavierStokes:
             self._h = None
 
 
-def step_graph(states, uks):
+def step_graph(states, uks, batched=True):
     """A library-owned CUDA graph of one RK4 step of every field (states[i]
-    advances uks[i]), each transform of all fields batched into one launch per
-    stage; ``launch(stream)`` advances all fields by one step."""
+    advances uks[i]); ``batched``: each transform of all fields batched into
+    one launch per stage, else each field's step on one of up to four
+    concurrent branches.  ``launch(stream)`` advances all fields by one step."""
     n = len(states)
     if len(uks) != n or n == 0:
         raise ValueError("one spectral buffer per state")
     st = (ctypes.c_void_p * n)(*[s._h.value for s in states])
     bufs = (ctypes.c_void_p * n)(*[_ptr(u).value for u in uks])
     h = ctypes.c_void_p()
-    _check(lib.dfft_ns_graph_create(ctypes.byref(h), st, bufs, n))
+    _check(lib.dfft_ns_graph_create(ctypes.byref(h), st, bufs, n, 1 if batched else 0))
     return Graph._from_handle(h, list(states) + [s._plan for s in states])

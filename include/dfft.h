@@ -248,13 +248,18 @@ dfft_status dfft_ns_step(dfft_ns* ns, void* uk, void* stream);
  * (factor 1 on kz = 0, else 2), FP64 reduction; synchronises the stream */
 dfft_status dfft_ns_energy(dfft_ns* ns, const void* uk, double* energy, void* stream);
 /* One RK4 time step of `count` fields (distinct states, uks[i] the spectral
- * buffer of states[i]) captured once into a library-owned CUDA graph: per RK
- * stage the pointwise phases per field and every transform of all fields
- * through one batched execution (one launch per stage of the transform).
+ * buffer of states[i]) captured once into a library-owned CUDA graph.
+ *   batched = 1: per RK stage the pointwise phases per field and every
+ *     transform of all fields through one batched execution (one launch per
+ *     stage of the transform; the states' plans must be distinct);
+ *   batched = 0: each field's step on one of up to four concurrent graph
+ *     branches with its plan's tuned kernels (fields sharing a plan on one
+ *     branch).
  * dfft_graph_launch advances every field by one step; dfft_graph_destroy
  * frees it.  States and plans must outlive the graph.  No counterpart in the
  * reference (main.cpp:518-586 loops over the fields' RK4 stages). */
-dfft_status dfft_ns_graph_create(dfft_graph** graph, dfft_ns* const* states, void* const* uks, int64_t count);
+dfft_status dfft_ns_graph_create(dfft_graph** graph, dfft_ns* const* states, void* const* uks, int64_t count,
+                                 int32_t batched);
 /* Physical velocity of a spectrum (the backward transform of diag_fields,
  * main.cpp:711-724) into a buffer of the plan's input layout; uk is not
  * modified. */

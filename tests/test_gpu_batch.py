@@ -93,8 +93,9 @@ def test_batch_rejects_bad_sets():
             dfft.Batch(plans)
 
 
+@pytest.mark.parametrize("batched", [True, False])
 @pytest.mark.parametrize("precision", ["float64", "float32"])
-def test_navier_stokes_step_graph(precision):
+def test_navier_stokes_step_graph(precision, batched):
     import torch
     cdt = torch.complex128 if precision == "float64" else torch.complex64
     tol = 1e-12 if precision == "float64" else 1e-5
@@ -111,7 +112,7 @@ def test_navier_stokes_step_graph(precision):
         # per-field reference: its own state object on a copy
         s2 = dfft.NavierStokes(p, nu=0.01, dt=0.01, lx=2.0)
         refs.append((s2, uk.clone()))
-    g = dfft.step_graph(states, uks)
+    g = dfft.step_graph(states, uks, batched=batched)
     for _ in range(3):
         g.launch()
         for s2, r in refs:

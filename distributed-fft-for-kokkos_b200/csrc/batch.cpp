@@ -35,7 +35,8 @@ Batch::Batch(std::vector<const Plan*> plans) : plans_(std::move(plans)) {
     if (p->desc().exec_mode != 0) fail(kErrInvalidArgument, "batched execution needs fused plans");
     for (bool fwd : {true, false})
       for (const Op& op : p->program(fwd))
-        if (op.type != Op::Stage) fail(kErrInvalidArgument, "batched execution needs fused plans");
+        if (op.type != Op::Stage)
+          fail(kErrInvalidArgument, "batched execution needs fused plans whose stages are all FFT stage kernels");
   }
   dbl_ = plans_[0]->desc().dbl;
   for (const Plan* p : plans_)

@@ -150,6 +150,32 @@ bool batch_stage_supported(int n);
 int batch_stage_lines(int n);
 // kind: kC2C, kR2C or kC2R (R2C / C2R: lines along a on both sides)
 cudaError_t launch_fft_batch(BatchParams& P, bool dbl, int kind, bool inverse, bool afast, cudaStream_t st);
+// Chirp-z (Bluestein) stage for line lengths the radix passes do not cover
+// (a prime factor above 13): X_k = c_k sum_j (x_j c_j) conj(c_{k-j}),
+// c_j = exp(-i pi j^2 / n) (conjugated for the inverse), as a circular
+// convolution of length m >= 2n - 1 through two m-point FFTs (bluestein.cu).
+//   pre:  z[line][j] = x_j c_j (j < n), 0 (n <= j < m), x read through the
+//         stage's source layout (R2C: real x; C2R: the full line rebuilt from
+//         the half spectrum, imaginary parts of DC / Nyquist dropped)
+//   mul:  z[line][k] *= filter[k] (the m-point FFT of the conjugate chirp,
+//         divided by m, so that the unnormalised inverse FFT gives the
+//         convolution)
+//   post: X_k = c_k z[line][k] * scale written through the stage's
+//         destination layout (R2C: k <= n/2; C2R: real parts)
+// Lines are the stage's (b, o0, o1) coordinates, line = ib + Eb (io0 + Eo0 io1).
+struct BlueArgs {
+  StageArgs S;         // stage geometry (layouts, axes, extents, n, kind via `kind`)
+  int kind;            // kC2C, kR2C or kC2R
+  int inverse;
+  int m;
+  long long nlines;
+  const void* chirp;   // n complex values exp(-i pi (j^2 mod 2n) / n) of the stage precision
+  const void* filter;  // m complex values
+  const void* zin;     // post: z (nlines x m complex)
+  void* zout;          // pre: z
+};
+// op: 0 pre, 1 mul (on zout), 2 post
+cudaError_t launch_bluestein(int op, const BlueArgs& B, bool dbl, cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);
 cudaError_t launch_scale(void* p, int64_t n_real, bool dbl, double s, cudaStream_t st);

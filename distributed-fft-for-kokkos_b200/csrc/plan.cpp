@@ -76,6 +76,53 @@ std::vector<int> radix_plan(std::size_t n) {
   return r;
 }
 
+// Whether radix_plan covers n (prime factors up to 13, few enough passes).
+bool radix_supported(std::size_t n) {
+  if (n == 0) return false;
+  std::size_t m = n;
+  int k2 = 0;
+  while (m % 2 == 0) {
+    m /= 2;
+    ++k2;
+  }
+  int passes = k2 / 3 + (k2 % 3 != 0 ? 1 : 0);  // the radix-8 / 4 / 2 passes of radix_plan
+  for (std::size_t p : {3, 5, 7, 11, 13})
+    while (m % p == 0) {
+      m /= p;
+      ++passes;
+    }
+  return m == 1 && passes <= dev::kMaxPasses;
+}
+
+// In-place radix-2 FFT (exp(-2 pi i jk / m)) of m = 2^k long double values.
+void host_fft(std::vector<long double>& re, std::vector<long double>& im) {
+  const std::size_t m = re.size();
+  for (std::size_t i = 1, j = 0; i < m; ++i) {
+    std::size_t bit = m >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      std::swap(re[i], re[j]);
+      std::swap(im[i], im[j]);
+    }
+  }
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (std::size_t len = 2; len <= m; len <<= 1) {
+    for (std::size_t k = 0; k < len / 2; ++k) {
+      const long double ang = -2.0L * pi * static_cast<long double>(k) / static_cast<long double>(len);
+      const long double wr = cosl(ang), wi = sinl(ang);
+      for (std::size_t i = k; i < m; i += len) {
+        const std::size_t j = i + len / 2;
+        const long double xr = re[j] * wr - im[j] * wi, xi = re[j] * wi + im[j] * wr;
+        re[j] = re[i] - xr;
+        im[j] = im[i] - xi;
+        re[i] += xr;
+        im[i] += xi;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -103,6 +150,8 @@ Plan::Plan(const PlanDesc& d, bool on_device) : d_(d), on_device_(on_device) {
     for (auto& kv : twiddles_) cudaFree(kv.second);
     if (d_tables_) cudaFree(d_tables_);
     if (d_err_) cudaFree(d_err_);
+    for (auto& kv : blue_tables_)
+      for (void* p : kv.second) cudaFree(p);
     throw;
   }
 }
@@ -113,6 +162,8 @@ Plan::~Plan() {
   for (auto& kv : twiddles_) cudaFree(kv.second);
   if (d_tables_) cudaFree(d_tables_);
   if (d_err_) cudaFree(d_err_);
+  for (auto& kv : blue_tables_)
+    for (void* p : kv.second) cudaFree(p);
 }
 
 void Plan::analyze() {
@@ -278,6 +329,114 @@ const void* Plan::twiddle(std::size_t n) {
   return p;
 }
 
+// Chirp and filter tables of an n-point chirp-z stage with m-point FFTs, in
+// the plan's precision: chirp c_j = exp(-i pi (j^2 mod 2n) / n), j < n; the
+// forward filter is FFT_m(b) / m with b_j = conj(c_j) for j < n, b_{m-j} = b_j
+// for 0 < j < n and 0 elsewhere, the inverse filter the same for the
+// conjugate chirp.  Computed in long double on the host.
+void Plan::bluestein_tables(std::size_t n, std::size_t m, const void** chirp, const void** ffwd, const void** finv) {
+  auto key = std::make_pair(n, m);
+  auto it = blue_tables_.find(key);
+  if (it == blue_tables_.end()) {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<long double> cr(n), ci(n);
+    for (std::size_t j = 0; j < n; ++j) {
+      const unsigned long long q = (static_cast<unsigned long long>(j) * j) % (2ull * n);
+      const long double ang = -pi * static_cast<long double>(q) / static_cast<long double>(n);
+      cr[j] = cosl(ang);
+      ci[j] = sinl(ang);
+    }
+    std::vector<std::vector<long double>> tabs;  // chirp (re, im interleaved), filters
+    std::vector<long double> ch(2 * n);
+    for (std::size_t j = 0; j < n; ++j) {
+      ch[2 * j] = cr[j];
+      ch[2 * j + 1] = ci[j];
+    }
+    tabs.push_back(ch);
+    for (int dir = 0; dir < 2; ++dir) {
+      // forward chirp c: b = conj(c); inverse chirp conj(c): b = c
+      std::vector<long double> br(m, 0.0L), bi(m, 0.0L);
+      for (std::size_t j = 0; j < n; ++j) {
+        const long double im = dir == 0 ? -ci[j] : ci[j];
+        br[j] = cr[j];
+        bi[j] = im;
+        if (j > 0) {
+          br[m - j] = cr[j];
+          bi[m - j] = im;
+        }
+      }
+      host_fft(br, bi);
+      std::vector<long double> f(2 * m);
+      for (std::size_t k = 0; k < m; ++k) {
+        f[2 * k] = br[k] / static_cast<long double>(m);
+        f[2 * k + 1] = bi[k] / static_cast<long double>(m);
+      }
+      tabs.push_back(f);
+    }
+    std::vector<void*> ptrs;
+    for (auto& t : tabs) {
+      const std::size_t bytes = t.size() * (d_.dbl ? 8 : 4);
+      void* p = nullptr;
+      if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        for (void* q : ptrs) cudaFree(q);
+        fail(kErrAlloc, "cudaMalloc of chirp-z tables failed");
+      }
+      ptrs.push_back(p);
+      workspace_bytes_ += bytes;
+      cudaError_t e;
+      if (d_.dbl) {
+        std::vector<double> h(t.begin(), t.end());
+        e = cudaMemcpy(p, h.data(), bytes, cudaMemcpyHostToDevice);
+      } else {
+        std::vector<float> h(t.begin(), t.end());
+        e = cudaMemcpy(p, h.data(), bytes, cudaMemcpyHostToDevice);
+      }
+      if (e != cudaSuccess) {
+        for (void* q : ptrs) cudaFree(q);
+        fail(kErrCuda, std::string("chirp-z table upload: ") + cudaGetErrorString(e));
+      }
+    }
+    it = blue_tables_.emplace(key, ptrs).first;
+  }
+  *chirp = it->second[0];
+  *ffwd = it->second[1];
+  *finv = it->second[2];
+}
+
+void Plan::push_stage(std::vector<Op>& prog, const Op& op) {
+  if (!op.blue) {
+    prog.push_back(op);
+    return;
+  }
+  const std::size_t nl = static_cast<std::size_t>(op.blue_lines), m = static_cast<std::size_t>(op.blue_m);
+  Layout Z;
+  Z.gext = {nl, m};
+  Z.topo = {1, 1};
+  Z.map = identity_map(2);
+  Z.view_right = true;
+  Z.complex = true;
+  const int lz = add_layout(Z);
+  const std::size_t zb = nl * m * (d_.dbl ? 16 : 8);
+  const int z1 = debug_buffer(-2, 0, 0, zb), z2 = debug_buffer(-2, 0, 1, zb);
+  Op pre = op;
+  pre.type = Op::BluePre;
+  pre.dst = z1;
+  Op f1 = make_stage(lz, lz, 1, dev::kC2C, false, 1.0);
+  f1.src = z1;
+  f1.dst = z2;
+  Op mul = op;
+  mul.type = Op::BlueMul;
+  mul.src = mul.dst = z2;
+  Op f2 = make_stage(lz, lz, 1, dev::kC2C, true, 1.0);
+  f2.src = z2;
+  f2.dst = z1;
+  Op post = op;
+  post.type = Op::BluePost;
+  post.src = z1;
+  for (const Op* o : {&pre, &f1, &mul, &f2, &post}) prog.push_back(*o);
+}
+
 Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse, double scale) {
   const Layout& S = layouts_[src_l];
   const Layout& Dl = layouts_[dst_l];
@@ -327,6 +486,20 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   A.store_afast = fd == a ? 1 : 0;
   A.scale = scale;
 
+  if (!is_copy && !radix_supported(n)) {
+    // chirp-z stage: a circular convolution of length m >= 2n - 1
+    std::size_t m = 1;
+    while (m < 2 * n - 1) m <<= 1;
+    op.blue = true;
+    op.blue_m = static_cast<int>(m);
+    op.blue_lines = static_cast<long long>(A.Eb) * A.Eo0 * A.Eo1;
+    const void *chirp = nullptr, *ffwd = nullptr, *finv = nullptr;
+    bluestein_tables(n, m, &chirp, &ffwd, &finv);
+    op.blue_chirp = chirp;
+    op.blue_filter = inverse ? finv : ffwd;
+    op.tiles = 1;
+    return op;
+  }
   if (!is_copy) {
     auto radices = radix_plan(n);
     A.npass = static_cast<int>(radices.size());
@@ -618,7 +791,7 @@ void Plan::build_fused(bool forward) {
     Op op = make_stage(src_l, dst_l, order[s], kind, !forward, last ? (forward ? scale_fwd_ : scale_bwd_) : 1.0);
     op.src = first ? kBufIn : (((s - 1) % 2 == 0) ? kBufScratch0 : kBufScratch1);
     op.dst = last ? kBufOut : ((s % 2 == 0) ? kBufScratch0 : kBufScratch1);
-    prog.push_back(op);
+    push_stage(prog, op);
   }
 }
 
@@ -675,7 +848,7 @@ void Plan::build_adjoint(bool of_forward) {
       Op op = make_stage(cur_l, dst_l, order[s], kind, true, last ? scale : 1.0);
       op.src = cur_b;
       op.dst = last ? kBufOut : (cur_b == kBufScratch0 ? kBufScratch1 : kBufScratch0);
-      prog.push_back(op);
+      push_stage(prog, op);
       cur_l = dst_l;
       cur_b = op.dst;
       if (s == 0 && d_.r2c && S >= 2) prog.push_back(weight_op(li, cur_b, 0.5));
@@ -690,7 +863,7 @@ void Plan::build_adjoint(bool of_forward) {
       Op op = make_stage(cur_l, dst_l, order[s], kind, false, last ? scale : 1.0);
       op.src = cur_b;
       op.dst = last ? kBufOut : (cur_b == kBufScratch0 ? kBufScratch1 : kBufScratch0);
-      prog.push_back(op);
+      push_stage(prog, op);
       cur_l = dst_l;
       cur_b = op.dst;
       if (first && d_.r2c) prog.push_back(weight_op(cur_l, cur_b, 2.0));
@@ -759,7 +932,7 @@ void Plan::build_literal(bool forward) {
     op.src = cur_b;
     // in place on scratch; out of place when reading the caller's buffer or changing type
     op.dst = (cur_b == kBufIn || kind == dev::kR2C || kind == dev::kC2R) ? other_scratch(cur_b) : cur_b;
-    prog.push_back(op);
+    push_stage(prog, op);
     cur_l = nl;
     cur_b = op.dst;
   };
@@ -978,7 +1151,7 @@ void Plan::allocate_device() {
   for (auto* progs : {&prog_[0], &prog_[1], &adj_[0], &adj_[1]}) {
     for (auto& op : *progs) {
       if (op.type == Op::Weight) op.sa.dst = dev_layout(op.src_layout);
-      if (op.type == Op::Stage) {
+      if (op.type == Op::Stage || op.type == Op::BluePre || op.type == Op::BluePost) {
         op.sa.src = dev_layout(op.src_layout);
         op.sa.dst = dev_layout(op.dst_layout);
         op.sa.err = d_err_;
@@ -1030,8 +1203,6 @@ void Plan::autotune() {
   if (env && std::string(env) == "0") return;
   if (bufs_.size() <= kBufScratch1 || !bufs_[kBufScratch0] || !bufs_[kBufScratch1]) return;
   cudaStream_t st = d_.stream;
-  void* s0 = bufs_[kBufScratch0];
-  void* s1 = bufs_[kBufScratch1];
   bool cleared = false;
   std::lock_guard<std::mutex> lock(g_tune_mutex);
   load_tune_cache_locked();
@@ -1040,6 +1211,19 @@ void Plan::autotune() {
       if (op.type != Op::Stage || !op.fast) continue;
       dev::StageArgs& A = op.sa;
       if (A.src_line_affine || A.dst_line_affine) continue;  // general layouts keep the default tile
+      // Trial buffers: the op's own plan-owned buffers, else the scratch
+      // pair; each must hold the whole layout the stage reads / writes
+      // (chirp-z stages run their FFTs on arrays larger than the scratch).
+      auto elem_bytes = [&](int l) { return layouts_[l].complex ? (d_.dbl ? 16u : 8u) : (d_.dbl ? 8u : 4u); };
+      const std::size_t need_in = layout_elements(layouts_[op.src_layout]) * elem_bytes(op.src_layout);
+      const std::size_t need_out = layout_elements(layouts_[op.dst_layout]) * elem_bytes(op.dst_layout);
+      const int tin = op.src >= kBufScratch0 ? op.src : kBufScratch0;
+      int tout = op.dst >= kBufScratch0 ? op.dst : kBufScratch1;
+      if (tout == tin && op.src != op.dst) tout = tin == kBufScratch0 ? kBufScratch1 : kBufScratch0;
+      if (!bufs_.at(tin) || !bufs_.at(tout) || buf_bytes_.at(tin) < need_in || buf_bytes_.at(tout) < need_out)
+        continue;  // no trial buffers large enough: keep the default tile
+      void* t_in = bufs_[tin];
+      void* t_out = bufs_[tout];
       std::ostringstream k;
       const bool real = op.kind == dev::kR2C || op.kind == dev::kC2R;  // two real lines per register line
       const bool pair_ok = op.single_B != 0;                            // eligible for two lines per thread
@@ -1081,8 +1265,9 @@ void Plan::autotune() {
         continue;
       }
       if (!cleared) {
-        cuda_check(cudaMemsetAsync(s0, 0, buf_bytes_[kBufScratch0], st), "tuner clear");
-        cuda_check(cudaMemsetAsync(s1, 0, buf_bytes_[kBufScratch1], st), "tuner clear");
+        // every plan-owned buffer starts cleared (trial launches read them)
+        for (std::size_t i = kBufScratch0; i < bufs_.size(); ++i)
+          if (bufs_[i]) cuda_check(cudaMemsetAsync(bufs_[i], 0, buf_bytes_[i], st), "tuner clear");
         cleared = true;
       }
       std::vector<int> cand;
@@ -1115,8 +1300,8 @@ void Plan::autotune() {
       for (int code : cand) {
         apply(code);
         dev::StageArgs T = A;
-        T.in = s0;
-        T.out = s1;
+        T.in = t_in;
+        T.out = t_out;
         if (launch_stage(op, T, st) != cudaSuccess) {
           cudaGetLastError();
           continue;
@@ -1171,6 +1356,33 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
         X.dst = buf(op0.dst);
         if (X.bufsize * X.nprocs == 0) break;
         e = dev::launch_xpose(op0.type == Op::Pack ? 0 : (op0.type == Op::All2All ? 1 : 2), X, op0.elem_bytes, stream);
+        break;
+      }
+      case Op::BluePre:
+      case Op::BlueMul:
+      case Op::BluePost: {
+        dev::BlueArgs B;
+        std::memset(&B, 0, sizeof(B));
+        B.S = op0.sa;
+        B.kind = op0.kind;
+        B.inverse = op0.inverse ? 1 : 0;
+        B.m = op0.blue_m;
+        B.nlines = op0.blue_lines;
+        B.chirp = op0.blue_chirp;
+        B.filter = op0.blue_filter;
+        int which = 0;
+        if (op0.type == Op::BluePre) {
+          B.S.in = buf(op0.src);
+          B.zout = buf(op0.dst);
+        } else if (op0.type == Op::BlueMul) {
+          which = 1;
+          B.zout = buf(op0.dst);
+        } else {
+          which = 2;
+          B.zin = buf(op0.src);
+          B.S.out = buf(op0.dst);
+        }
+        e = dev::launch_bluestein(which, B, d_.dbl, stream);
         break;
       }
       case Op::Scale: e = dev::launch_scale(buf(op0.dst), op0.n_real, d_.dbl, op0.scale, stream); break;

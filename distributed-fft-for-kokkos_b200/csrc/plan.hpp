@@ -50,7 +50,7 @@ struct TmaSource {
 bool tma_encode(void* map, const void* base, const TmaSource& t);
 
 struct Op {
-  enum Type { Stage, Pack, All2All, Unpack, Scale, Copy, Weight } type;
+  enum Type { Stage, Pack, All2All, Unpack, Scale, Copy, Weight, BluePre, BlueMul, BluePost } type;
   int src = -1, dst = -1;  // buffer ids
   // Stage
   dev::StageArgs sa{};
@@ -62,6 +62,13 @@ struct Op {
   int pair_B = 0;     // lines per tile of the two-line kernel, for TMA stages whose source
                       // cannot be described by a tensor map at run time
   TmaSource tma;      // source description of a TMA-eligible b-fast pair stage
+  // chirp-z stage (line length with a prime factor above 13): make_stage marks
+  // it, push_stage expands it into pre / FFT / mul / inverse FFT / post ops
+  bool blue = false;
+  int blue_m = 0;
+  long long blue_lines = 0;
+  const void* blue_chirp = nullptr;
+  const void* blue_filter = nullptr;
   int nthreads = 256;
   std::size_t smem = 0;
   unsigned tiles = 0;
@@ -153,6 +160,10 @@ class Plan {
   std::vector<std::size_t> fft_axis_order() const;
   Layout block_layout(const Ext& topo, bool rank_right, const Ext& map, bool complex) const;
   Op make_stage(int src_layout, int dst_layout, std::size_t a, int kind, bool inverse, double scale);
+  // Append a stage op, or the five ops of a chirp-z stage.
+  void push_stage(std::vector<Op>& prog, const Op& op);
+  std::map<std::pair<std::size_t, std::size_t>, std::vector<void*>> blue_tables_;  // (n, m) -> chirp, filter fwd / inv
+  void bluestein_tables(std::size_t n, std::size_t m, const void** chirp, const void** ffwd, const void** finv);
   std::int64_t add_geo(const Layout& L, const BlockInfo& b, std::size_t pc);
   void build_fused(bool forward);
   void build_literal(bool forward);

@@ -167,3 +167,17 @@ def spectrum(uk, lx, shape, num_bins=50):
         m = (k_mag >= bins[i]) & (k_mag < bins[i + 1])
         spec[i] = float(np.sum(ek[m]))
     return spec, 0.5 * (bins[:-1] + bins[1:])
+
+
+def energy_with_block_local_factor(uk, lx, shape, z_blocks):
+    """The example's diag_energy sum with its factor taken by the local z
+    index of each output block (main.cpp:741-766: factor 1 where the block's
+    local i2 == 0): z_blocks lists the (start, extent) of the z bins of the
+    output topology.  Equal to ``energy`` when z is not split."""
+    nx, ny, nz = shape
+    n = float(nx) * ny * nz
+    factor = np.full(uk.shape[-1], 2.0)
+    for start, _ in z_blocks:
+        factor[start] = 1.0
+    e = 0.5 * factor[None, None, None, :] * (uk.real ** 2 + uk.imag ** 2)
+    return float(np.sum(e) * (lx * np.pi) ** 3 / (n * n))

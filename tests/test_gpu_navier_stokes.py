@@ -205,3 +205,27 @@ def test_ns_write_diagnostics_files(tmp_path, precision):
     assert {p.name for p in tmp_path.iterdir()} == names
     assert abs(d["energy"] / N.energy(y, lx, shape) - 1.0) <= 1e-12
     assert abs(d["enstrophy"] / (3.0 * d["energy"]) - 1.0) <= tol
+
+
+@pytest.mark.parametrize("n,tin,tout", [
+    (64, (1, 2, 2, 1), (1, 1, 2, 2)),   # the example's decomposition, px = py = 2
+    (96, (1, 4, 1, 1), (1, 1, 4, 1)),   # its slab form (py = 1)
+    (96, (1, 2, 3, 1), (1, 1, 2, 3)),
+])
+def test_ns_at_the_reference_decomposition(n, tin, tout):
+    """The solver on the example's own decomposition (1, px, py, 1) ->
+    (1, 1, px, py) at cfg3 grid sizes, FP64, against the oracle: one
+    right-hand side and one RK4 step of a random divergence-free field."""
+    import torch
+    shape, lx, nu, dt = (n, n, n), 2.0, 1.0 / 1600.0, 1e-3
+    plan, cdt = _setup(shape, tin, tout, "float64")
+    ns = dfft.NavierStokes(plan, nu=nu, dt=dt, lx=lx)
+    y = _random_spectrum(shape, 12, lx) / n ** 1.5
+    uk = _to_dev(plan, y, cdt)
+    dukdt = torch.empty_like(uk)
+    ns.rhs(uk, dukdt)
+    _, ref_r = N.rhs(y, nu, lx, shape)
+    assert _rel(_to_host(plan, dukdt), ref_r) <= 1e-12
+    uk = _to_dev(plan, y, cdt)
+    ns.step(uk)
+    assert _rel(_to_host(plan, uk), N.rk4_step(y, nu, dt, lx, shape)) <= 1e-12

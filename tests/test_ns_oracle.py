@@ -88,3 +88,22 @@ def test_spectrum_bins_follow_the_reference():
     ek = 0.5 * f[None, None, :] * np.sum(np.abs(uk) ** 2, axis=0)
     assert abs(float(np.sum(spec)) - float(np.sum(ek[km < km.max()]))) < 1e-9 * float(np.sum(ek))
     assert np.allclose(kv, (np.arange(7) + 0.5) * km.max() / 7, rtol=0, atol=1e-12)
+
+
+def test_energy_factor_at_the_reference_decomposition():
+    """The example takes the Hermitian factor of its energy by the local z
+    index of each rank's output block; at out_topology (1, 1, px, 1) (z not
+    split) that is the global kz = 0 plane and the two sums agree exactly; with
+    z split (py > 1) the example weights the first plane of every z block by 1
+    instead of 2, so its diagnostic differs from the energy by that plane's
+    share (the solver itself is unaffected)."""
+    shape, lx = (16, 16, 16), 2.0
+    rng = np.random.default_rng(9)
+    k, _, inv_ksq = N.wavenumbers(*shape, lx)
+    uk = N.projection(np.fft.rfftn(rng.standard_normal((3,) + shape), axes=(1, 2, 3)), k, inv_ksq)
+    e = N.energy(uk, lx, shape)
+    assert N.energy_with_block_local_factor(uk, lx, shape, [(0, 9)]) == e
+    z_split = [(0, 5), (5, 4)]  # 9 half-spectrum planes over py = 2 (first n % P bins larger)
+    e_blocks = N.energy_with_block_local_factor(uk, lx, shape, z_split)
+    plane = 0.5 * np.sum(np.abs(uk[..., 5]) ** 2) * (lx * np.pi) ** 3 / float(16 ** 3) ** 2
+    assert abs((e - e_blocks) - plane) <= 1e-12 * e

@@ -1,6 +1,8 @@
 // Chirp-z (Bluestein) stage kernels: the gather / chirp, filter and chirp /
-// scatter steps around two m-point FFTs (see BlueArgs in dev_types.h).  The
-// FFTs themselves are ordinary register stages on a plain (lines, m) array.
+// scatter steps around two m-point FFTs (see BlueArgs in dev_types.h); the
+// same gather / scatter (without chirp) and a twiddle step serve the
+// four-step stages of lines too long for one stage.  The FFTs themselves are
+// ordinary register or generic stages on a plain (lines, m) array.
 // These kernels address the rank-blocked layouts element by element through
 // the layout tables: the path serves line lengths the radix passes cannot
 // (a prime factor above 13), not the hot shapes.
@@ -12,6 +14,7 @@ namespace {
 
 template <typename T>
 __device__ __forceinline__ cplx<T> chirp_at(const BlueArgs& B, int j) {
+  if (B.four_n1 > 0) return mk<T>(T(1), T(0));  // four-step: plain copy
   cplx<T> c = reinterpret_cast<const cplx<T>*>(B.chirp)[j];
   if (B.inverse) c.y = -c.y;
   return c;
@@ -72,6 +75,24 @@ __global__ void blue_mul_kernel(const BlueArgs B) {
     z[i] = cmul(z[i], f[i % B.m]);
 }
 
+// four-step twiddle: z[line][k2][j1] *= w_n^(j1 k2)
+template <typename T>
+__global__ void four_twiddle_kernel(const BlueArgs B) {
+  using C = cplx<T>;
+  const int n = B.S.n, n1 = B.four_n1;
+  const long long total = B.nlines * n;
+  C* z = reinterpret_cast<C*>(B.zout);
+  const C* tw = reinterpret_cast<const C*>(B.tw);
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int p = static_cast<int>(i % n);
+    const long long j1 = p % n1, k2 = p / n1;
+    C w = tw[(j1 * k2) % n];
+    if (B.inverse) w.y = -w.y;
+    z[i] = cmul(z[i], w);
+  }
+}
+
 template <typename T>
 __global__ void blue_post_kernel(const BlueArgs B) {
   using C = cplx<T>;
@@ -85,7 +106,8 @@ __global__ void blue_post_kernel(const BlueArgs B) {
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
     const long long line = i / nout;
     const int k = static_cast<int>(i % nout);
-    const C v = cscale(cmul(z[line * m + k], chirp_at<T>(B, k)), sc);
+    const long long src = B.four_n1 > 0 ? (k % B.four_n2) * static_cast<long long>(B.four_n1) + k / B.four_n2 : k;
+    const C v = cscale(cmul(z[line * m + src], chirp_at<T>(B, k)), sc);
     int c[4];
     line_coords(S, line, c);
     c[S.a] = k;
@@ -112,15 +134,17 @@ cudaError_t launch_t(int op, const BlueArgs& B, cudaStream_t st) {
     blue_pre_kernel<T><<<grid_for(work), 256, 0, st>>>(B);
   else if (op == 1)
     blue_mul_kernel<T><<<grid_for(work), 256, 0, st>>>(B);
-  else
+  else if (op == 2)
     blue_post_kernel<T><<<grid_for(work), 256, 0, st>>>(B);
+  else
+    four_twiddle_kernel<T><<<grid_for(work), 256, 0, st>>>(B);
   return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_bluestein(int op, const BlueArgs& B, bool dbl, cudaStream_t st) {
-  if (op < 0 || op > 2) return cudaErrorInvalidValue;
+  if (op < 0 || op > 3) return cudaErrorInvalidValue;
   return dbl ? launch_t<double>(op, B, st) : launch_t<float>(op, B, st);
 }
 

@@ -173,8 +173,15 @@ struct BlueArgs {
   const void* filter;  // m complex values
   const void* zin;     // post: z (nlines x m complex)
   void* zout;          // pre: z
+  // four-step mode (four_n1 > 0; lines too long for one stage, n = n1 n2):
+  // pre copies the line without chirp (m = n), z viewed as (line, j2, j1)
+  // with j = j1 + n1 j2; twiddle multiplies z[line][k2][j1] by
+  // w_n^(j1 k2) (tw: the n-point table exp(-2 pi i k / n), conjugated for
+  // the inverse); post reads X_k at (k mod n2) n1 + k / n2
+  int four_n1, four_n2;
+  const void* tw;
 };
-// op: 0 pre, 1 mul (on zout), 2 post
+// op: 0 pre, 1 mul (on zout), 2 post, 3 four-step twiddle (on zout)
 cudaError_t launch_bluestein(int op, const BlueArgs& B, bool dbl, cudaStream_t st);
 // op: 0 pack, 1 all-to-all, 2 unpack
 cudaError_t launch_xpose(int op, const XposeArgs& X, int elem_bytes, cudaStream_t st);

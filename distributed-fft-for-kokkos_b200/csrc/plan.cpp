@@ -405,6 +405,42 @@ void Plan::bluestein_tables(std::size_t n, std::size_t m, const void** chirp, co
 }
 
 void Plan::push_stage(std::vector<Op>& prog, const Op& op) {
+  if (op.four_n1 > 0) {
+    // four-step: z = the lines as (lines, n2, n1) arrays (j = j1 + n1 j2);
+    // FFT over j2, twiddle w_n^(j1 k2), FFT over j1, scatter k = k2 + n2 k1
+    const std::size_t nl = static_cast<std::size_t>(op.blue_lines);
+    const std::size_t n1 = static_cast<std::size_t>(op.four_n1), n2 = static_cast<std::size_t>(op.four_n2);
+    Layout Z;
+    Z.gext = {nl, n2, n1};
+    Z.topo = {1, 1, 1};
+    Z.map = identity_map(3);
+    Z.view_right = true;
+    Z.complex = true;
+    const int lz = add_layout(Z);
+    const std::size_t zb = nl * n1 * n2 * (d_.dbl ? 16 : 8);
+    const int z1 = debug_buffer(-3, 0, 0, zb), z2 = debug_buffer(-3, 0, 1, zb);
+    Op pre = op;
+    pre.type = Op::BluePre;
+    pre.dst = z1;
+    prog.push_back(pre);
+    Op f1 = make_stage(lz, lz, 1, dev::kC2C, op.inverse, 1.0);
+    f1.src = z1;
+    f1.dst = z2;
+    push_stage(prog, f1);
+    Op tw = op;
+    tw.type = Op::FourTwiddle;
+    tw.src = tw.dst = z2;
+    prog.push_back(tw);
+    Op f2 = make_stage(lz, lz, 2, dev::kC2C, op.inverse, 1.0);
+    f2.src = z2;
+    f2.dst = z1;
+    push_stage(prog, f2);
+    Op post = op;
+    post.type = Op::BluePost;
+    post.src = z1;
+    prog.push_back(post);
+    return;
+  }
   if (!op.blue) {
     prog.push_back(op);
     return;
@@ -422,19 +458,23 @@ void Plan::push_stage(std::vector<Op>& prog, const Op& op) {
   Op pre = op;
   pre.type = Op::BluePre;
   pre.dst = z1;
-  Op f1 = make_stage(lz, lz, 1, dev::kC2C, false, 1.0);
+  prog.push_back(pre);
+  Op f1 = make_stage(lz, lz, 1, dev::kC2C, false, 1.0);  // may itself be a four-step stage
   f1.src = z1;
   f1.dst = z2;
+  push_stage(prog, f1);
   Op mul = op;
   mul.type = Op::BlueMul;
   mul.src = mul.dst = z2;
+  prog.push_back(mul);
   Op f2 = make_stage(lz, lz, 1, dev::kC2C, true, 1.0);
   f2.src = z2;
   f2.dst = z1;
+  push_stage(prog, f2);
   Op post = op;
   post.type = Op::BluePost;
   post.src = z1;
-  for (const Op* o : {&pre, &f1, &mul, &f2, &post}) prog.push_back(*o);
+  prog.push_back(post);
 }
 
 Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse, double scale) {
@@ -521,7 +561,21 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   // shrink the tile to <= 100 KB of shared memory (pairs keep 2 lines)
   const std::size_t Bmin = pairs ? 2 : 1;
   while (B > Bmin && smem_for(B) > 100 * 1024) B = std::max(Bmin, B - (pairs ? 2 : 1));
-  if (smem_for(B) > 227 * 1024) fail(kErrUnsupported, "FFT length " + std::to_string(n) + " too large for one stage");
+  if (smem_for(B) > 227 * 1024) {
+    if (is_copy) fail(kErrUnsupported, "line of " + std::to_string(n) + " elements too large for one copy stage");
+    // four-step stage: n = n1 n2 with n1 the largest divisor <= sqrt(n)
+    std::size_t n1 = 1;
+    for (std::size_t d = 2; d * d <= n; ++d)
+      if (n % d == 0) n1 = d;
+    if (n1 == 1) fail(kErrUnsupported, "FFT length " + std::to_string(n) + " too large for one stage");
+    op.four_n1 = static_cast<int>(n1);
+    op.four_n2 = static_cast<int>(n / n1);
+    op.four_tw = twiddle(n);
+    op.blue_m = static_cast<int>(n);
+    op.blue_lines = static_cast<long long>(A.Eb) * A.Eo0 * A.Eo1;
+    op.tiles = 1;
+    return op;
+  }
   A.B = static_cast<int>(B);
   A.nl = static_cast<int>(pairs ? (B + 1) / 2 : B);
   A.pitch = static_cast<int>(pitch);
@@ -1360,7 +1414,8 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
       }
       case Op::BluePre:
       case Op::BlueMul:
-      case Op::BluePost: {
+      case Op::BluePost:
+      case Op::FourTwiddle: {
         dev::BlueArgs B;
         std::memset(&B, 0, sizeof(B));
         B.S = op0.sa;
@@ -1370,12 +1425,15 @@ void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, c
         B.nlines = op0.blue_lines;
         B.chirp = op0.blue_chirp;
         B.filter = op0.blue_filter;
+        B.four_n1 = op0.four_n1;
+        B.four_n2 = op0.four_n2;
+        B.tw = op0.four_tw;
         int which = 0;
         if (op0.type == Op::BluePre) {
           B.S.in = buf(op0.src);
           B.zout = buf(op0.dst);
-        } else if (op0.type == Op::BlueMul) {
-          which = 1;
+        } else if (op0.type == Op::BlueMul || op0.type == Op::FourTwiddle) {
+          which = op0.type == Op::BlueMul ? 1 : 3;
           B.zout = buf(op0.dst);
         } else {
           which = 2;

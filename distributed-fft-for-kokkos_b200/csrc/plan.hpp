@@ -50,7 +50,7 @@ struct TmaSource {
 bool tma_encode(void* map, const void* base, const TmaSource& t);
 
 struct Op {
-  enum Type { Stage, Pack, All2All, Unpack, Scale, Copy, Weight, BluePre, BlueMul, BluePost } type;
+  enum Type { Stage, Pack, All2All, Unpack, Scale, Copy, Weight, BluePre, BlueMul, BluePost, FourTwiddle } type;
   int src = -1, dst = -1;  // buffer ids
   // Stage
   dev::StageArgs sa{};
@@ -69,6 +69,11 @@ struct Op {
   long long blue_lines = 0;
   const void* blue_chirp = nullptr;
   const void* blue_filter = nullptr;
+  // four-step stage (a line too long for one stage, n = four_n1 * four_n2):
+  // pre / strided FFT / twiddle / contiguous FFT / post, sharing the chirp-z
+  // gather and scatter kernels
+  int four_n1 = 0, four_n2 = 0;
+  const void* four_tw = nullptr;
   int nthreads = 256;
   std::size_t smem = 0;
   unsigned tiles = 0;

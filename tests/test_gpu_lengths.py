@@ -1,8 +1,10 @@
-"""Line lengths with a prime factor above 13 (the chirp-z stage): C2C and
-R2C / C2R, slab and pencil, fused and literal programs, all four
-normalisations, and the adjoint identity, against the FP64 oracle
-(pocketfft handles any length).  Tolerances as everywhere: FP64 rel-L2 <=
-1e-12, FP32 <= 1e-6."""
+"""Line lengths outside the register and single-stage kernels: a prime
+factor above 13 (the chirp-z stage) and lines too long for one stage's
+shared memory (the four-step stage: FP64 8192, FP32 16384, and a chirp-z
+line whose own FFTs need the four-step stage).  C2C and R2C / C2R, slab and
+pencil, fused and literal programs, all four normalisations, and the adjoint
+identity, against the FP64 oracle (pocketfft handles any length).
+Tolerances as everywhere: FP64 rel-L2 <= 1e-12, FP32 <= 1e-6."""
 import numpy as np
 import pytest
 
@@ -60,3 +62,14 @@ def test_prime_length_adjoint_identity():
     lhs = float((fx.conj() * y).real.sum())
     rhs = float((x * fhy).sum())
     assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), 1.0)
+
+
+@pytest.mark.parametrize("gin,tin,tout,real,precision", [
+    ((8192, 4, 4), (1, 2, 1), (1, 1, 2), False, "float64"),
+    ((8192, 4, 4), (1, 2, 2), (2, 2, 1), True, "float64"),
+    ((4, 4, 8192), (2, 1, 1), (1, 2, 1), True, "float64"),     # the R2C axis itself
+    ((16384, 2, 4), (1, 2, 1), (1, 1, 2), False, "float32"),
+    ((4099, 3, 4), (1, 3, 1), (1, 1, 3), False, "float64"),   # prime: chirp-z with 8192-point four-step FFTs
+])
+def test_long_lines(gin, tin, tout, real, precision):
+    _roundtrip(gin, (0, 1, 2), tin, tout, real, precision)

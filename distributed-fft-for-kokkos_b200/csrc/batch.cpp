@@ -20,7 +20,9 @@ bool batchable(const Op& op) {
   return dev::batch_stage_supported(op.sa.n);
 }
 
-using GroupKey = std::tuple<int, bool, bool>;  // kind, inverse, a-fast rows
+// kind, inverse, a-fast rows, value class (3 * 2^k lengths or powers of two):
+// one batched launch per group
+using GroupKey = std::tuple<int, bool, bool, bool>;
 
 }  // namespace
 
@@ -53,7 +55,7 @@ std::size_t Batch::launches(bool forward) const {
       if (s >= prog.size() || prog[s].tiles == 0) continue;
       const Op& op = prog[s];
       if (batchable(op))
-        ++groups[GroupKey(op.kind, op.inverse, op.sa.load_afast != 0)];
+        ++groups[GroupKey(op.kind, op.inverse, op.sa.load_afast != 0, op.sa.n % 3 == 0)];
       else
         ++n;
     }
@@ -90,7 +92,7 @@ void Batch::execute(const void* const* ins, void* const* outs, bool forward, cud
       A.B = dev::batch_stage_lines(A.n);
       const int per = (op.kind == dev::kC2C) ? A.B : 2 * A.B;
       A.tiles_b = (A.Eb + per - 1) / per;
-      groups[GroupKey(op.kind, op.inverse, A.load_afast != 0)].push_back(A);
+      groups[GroupKey(op.kind, op.inverse, A.load_afast != 0, A.n % 3 == 0)].push_back(A);
     }
     for (auto& g : groups) {
       const auto& list = g.second;

@@ -135,8 +135,8 @@ int pair_tma_line_options(int n, int* opts);
 cudaError_t launch_fft_pair_tma(const StageArgs& A, const void* map, const TmaCoords& T, bool inverse,
                                 cudaStream_t st);
 // Batched register stage (fft_batch.cu): one persistent launch runs the same
-// stage (kind, direction, row orientation) of up to kMaxBatchFields fields of
-// any supported line lengths; field f owns work items prefix[f] .. prefix[f+1]
+// stage (kind, direction, row orientation) of up to kMaxBatchFields fields
+// whose line lengths share a value class (all powers of two, or all 3 * 2^k); field f owns work items prefix[f] .. prefix[f+1]
 // - 1, its tiles (tb + tiles_b (co0 + Eo0 co1)).  Every field's StageArgs
 // must have B = batch_stage_lines(n) (complex lines per tile) and the tiles_b
 // that goes with it; the args are taken by value (kernel parameter space).

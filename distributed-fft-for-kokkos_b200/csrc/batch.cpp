@@ -35,6 +35,7 @@ Batch::Batch(std::vector<const Plan*> plans) : plans_(std::move(plans)) {
     if (!seen.insert(p).second)
       fail(kErrInvalidArgument, "a plan appears twice in the batch (its scratch arrays would be shared)");
     if (p->desc().exec_mode != 0) fail(kErrInvalidArgument, "batched execution needs fused plans");
+    if (p->is_rank_plan()) fail(kErrInvalidArgument, "batched execution needs plans over all ranks, not per-rank plans");
     for (bool fwd : {true, false})
       for (const Op& op : p->program(fwd))
         if (op.type != Op::Stage)

@@ -98,15 +98,30 @@ const dfft::Plan& impl_of(const dfft_plan* p) {
   return *p->impl;
 }
 
+const dfft::Plan& rank_impl_of(const dfft_plan* p) {
+  const auto& impl = impl_of(p);
+  if (!impl.is_rank_plan())
+    dfft::fail(dfft::kErrInvalidArgument, "not a per-rank plan (dfft_plan_create_rank / dfft_plan_analyze_rank)");
+  return impl;
+}
+
+bool forward_of(int32_t direction) {
+  if (direction != DFFT_FORWARD && direction != DFFT_BACKWARD)
+    dfft::fail(dfft::kErrInvalidArgument, "Invalid FFT direction specified.");
+  return direction == DFFT_FORWARD;
+}
+
 void copy_ext(const dfft::Ext& e, uint64_t* dst, std::size_t n) {
   for (std::size_t i = 0; i < n; ++i) dst[i] = i < e.size() ? e[i] : 0;
 }
 
-dfft_status create(dfft_plan** out, const dfft_plan_desc* desc, bool on_device) {
+dfft_status create(dfft_plan** out, const dfft_plan_desc* desc, bool on_device, int64_t rank = -1) {
   return guarded([&] {
     if (!out) dfft::fail(dfft::kErrInvalidArgument, "null output pointer");
     *out = nullptr;
     auto p = to_desc(desc);
+    if (rank < -1) dfft::fail(dfft::kErrInvalidArgument, "rank must be non-negative");
+    p.rank = rank;
     auto* impl = new dfft::Plan(p, on_device);
     *out = new dfft_plan_s{impl};
   });
@@ -304,6 +319,80 @@ dfft_status dfft_get_max_buffer_size(const dfft_plan* plan, uint64_t* size) {
   return guarded([&] {
     if (!size) dfft::fail(dfft::kErrInvalidArgument, "null output");
     *size = impl_of(plan).max_buffer_size();
+  });
+}
+
+dfft_status dfft_plan_create_rank(dfft_plan** plan, const dfft_plan_desc* desc, int64_t rank) {
+  return create(plan, desc, true, rank);
+}
+
+dfft_status dfft_plan_analyze_rank(dfft_plan** plan, const dfft_plan_desc* desc, int64_t rank) {
+  return create(plan, desc, false, rank);
+}
+
+dfft_status dfft_get_num_exchanges(const dfft_plan* plan, int32_t direction, int64_t* n) {
+  return guarded([&] {
+    const auto& p = rank_impl_of(plan);
+    if (!n) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    *n = static_cast<int64_t>(p.exchanges(forward_of(direction)).size());
+  });
+}
+
+dfft_status dfft_get_exchange_info(const dfft_plan* plan, int32_t direction, int64_t k, dfft_exchange_info* info) {
+  return guarded([&] {
+    const auto& p = rank_impl_of(plan);
+    if (!info) dfft::fail(dfft::kErrInvalidArgument, "null output");
+    const auto& xs = p.exchanges(forward_of(direction));
+    if (k < 0 || static_cast<std::size_t>(k) >= xs.size())
+      dfft::fail(dfft::kErrInvalidArgument, "exchange index out of range");
+    const dfft::Exchange& x = xs[k];
+    info->block = static_cast<int64_t>(x.block);
+    info->comm_axis = x.comm_axis;
+    info->padded = x.padded ? 1 : 0;
+    info->elements = x.elements;
+    info->element_bytes = x.elem_bytes;
+    info->group_size = static_cast<int64_t>(x.group.members.size());
+  });
+}
+
+dfft_status dfft_get_exchange_group(const dfft_plan* plan, int32_t direction, int64_t k, int64_t rank,
+                                    int64_t* sub_rank, int64_t* members) {
+  return guarded([&] {
+    const auto& p = rank_impl_of(plan);
+    if (k < 0 || rank < 0) dfft::fail(dfft::kErrInvalidArgument, "negative index");
+    const dfft::ExchangeGroup g =
+        p.exchange_group_of(forward_of(direction), static_cast<std::size_t>(k), static_cast<std::size_t>(rank));
+    if (sub_rank) *sub_rank = static_cast<int64_t>(g.sub);
+    if (members)
+      for (std::size_t j = 0; j < g.members.size(); ++j) members[j] = static_cast<int64_t>(g.members[j]);
+  });
+}
+
+dfft_status dfft_execute_segment(const dfft_plan* plan, int32_t direction, int64_t segment, const void* in,
+                                 void* out, void* send, void* recv, void* stream) {
+  return guarded([&] {
+    const auto& p = rank_impl_of(plan);
+    if (segment < 0) dfft::fail(dfft::kErrInvalidArgument, "segment index out of range");
+    p.execute_segment(forward_of(direction), static_cast<std::size_t>(segment), in, out, send, recv,
+                      static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfft_status dfft_execute_exchanged(const dfft_plan* plan, const void* in, void* out, int32_t direction, void* send,
+                                   void* recv, dfft_exchange_fn exchange, void* user, void* stream) {
+  return guarded([&] {
+    const auto& p = rank_impl_of(plan);
+    const bool fwd = forward_of(direction);
+    const auto& xs = p.exchanges(fwd);
+    if (!xs.empty() && !exchange) dfft::fail(dfft::kErrInvalidArgument, "null exchange callback");
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (std::size_t s = 0; s <= xs.size(); ++s) {
+      p.execute_segment(fwd, s, in, out, send, recv, st);
+      if (s == xs.size()) break;
+      const uint64_t per_peer = xs[s].elements / xs[s].group.members.size() * xs[s].elem_bytes;
+      const int32_t rc = exchange(user, static_cast<int64_t>(s), send, recv, per_peer, stream);
+      if (rc != 0) dfft::fail(dfft::kErrCuda, "exchange callback returned " + std::to_string(rc));
+    }
   });
 }
 

@@ -11,7 +11,7 @@ std::vector<RankBlock> layout_blocks(const Layout& L) {
     b.coords = rank_to_coord(L.topo, r, L.rank_right);
     b.starts = compute_local_starts(L.gext, L.topo, r, L.rank_right);
     b.local = compute_local_extents(L.gext, L.topo, identity_map(D), r, L.rank_right);
-    b.mapped = compute_mapped_extents(b.local, L.map);
+    b.mapped = compute_mapped_extents(L.pad.empty() ? b.local : L.pad, L.map);
     b.stride.assign(D, 0);
     std::size_t s = 1;
     if (L.view_right) {
@@ -25,20 +25,26 @@ std::vector<RankBlock> layout_blocks(const Layout& L) {
         s *= b.mapped[i];
       }
     }
-    b.size = total_size(b.local);
+    b.size = total_size(L.pad.empty() ? b.local : L.pad);
     b.base = base;
     base += b.size;
   }
   return blocks;
 }
 
-std::size_t layout_elements(const Layout& L) { return total_size(L.gext); }
+std::size_t layout_elements(const Layout& L) {
+  return L.pad.empty() ? total_size(L.gext) : L.nprocs() * total_size(L.pad);
+}
 
-bool layout_separable(const Layout& L) {
+bool layout_even(const Layout& L) {
   for (std::size_t k = 0; k < L.gext.size(); ++k)
     if (L.topo[k] > 1 && L.gext[k] % L.topo[k] != 0) return false;
   return true;
 }
+
+// Padded blocks share one set of strides and one block size, so the offset
+// splits into per-axis terms even when the bins are ragged.
+bool layout_separable(const Layout& L) { return !L.pad.empty() || layout_even(L); }
 
 std::size_t layout_fast_axis(const Layout& L) { return L.view_right ? L.map.back() : L.map.front(); }
 

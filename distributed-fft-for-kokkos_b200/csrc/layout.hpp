@@ -7,7 +7,7 @@
 //
 // For the device, a layout becomes lookup tables:
 //   separable form (every rank has the same local extents, i.e. every split
-//   axis divides evenly): offset(c) = sum_k off_k[c_k];
+//   axis divides evenly, or padded blocks): offset(c) = sum_k off_k[c_k];
 //   general form (ragged bins):
 //     r = sum_k rk_k[c_k];  offset(c) = rbase[r] + sum_k loc_k[c_k] * rstride[r][k].
 #pragma once
@@ -28,11 +28,16 @@ struct Layout {
   Ext map;                 // local dim i <-> logical axis map[i]
   bool view_right = true;  // memory order of the local blocks
   bool complex = true;     // element type: complex or real
+  // Padded blocks (an exchange buffer of one rank): when not empty, every
+  // block is stored with these extents (logical axis order) instead of its
+  // own local extents, and block r starts at r * prod(pad); the entries past
+  // a block's local extents are padding that no kernel reads or writes.
+  Ext pad;
 
   std::size_t nprocs() const { return total_size(topo); }
   bool operator==(const Layout& o) const {
     return gext == o.gext && topo == o.topo && rank_right == o.rank_right && map == o.map &&
-           view_right == o.view_right && complex == o.complex;
+           view_right == o.view_right && complex == o.complex && pad == o.pad;
   }
   bool operator!=(const Layout& o) const { return !(*this == o); }
 };
@@ -47,10 +52,14 @@ struct RankBlock {
 };
 
 std::vector<RankBlock> layout_blocks(const Layout& L);
+// Elements of the buffer that holds the layout (padding included).
 std::size_t layout_elements(const Layout& L);
 bool layout_separable(const Layout& L);
 // Logical axis with unit stride (the fastest-varying axis of every block).
 std::size_t layout_fast_axis(const Layout& L);
+
+// Every split axis divides evenly (the blocks along it have equal extents).
+bool layout_even(const Layout& L);
 
 // Host image of the device tables of a layout, packed in one int64 array.
 struct LayoutTables {

@@ -130,8 +130,22 @@ void host_fft(std::vector<long double>& re, std::vector<long double>& im) {
 // ---------------------------------------------------------------------------
 Plan::Plan(const PlanDesc& d, bool on_device) : d_(d), on_device_(on_device) {
   analyze();
+  if (is_rank_plan()) {
+    if (static_cast<std::size_t>(d_.rank) >= nprocs())
+      fail(kErrInvalidArgument, "rank must be less than topology size.");
+    if (d_.exec_mode != 0) fail(kErrInvalidArgument, "per-rank plans run the fused execution mode only");
+    rank_exchanges(true);
+    rank_exchanges(false);
+  }
   if (!on_device_) return;
   try {
+    if (is_rank_plan()) {
+      build_rank(true);
+      build_rank(false);
+      allocate_device();
+      autotune();
+      return;
+    }
     build_fused(true);
     build_fused(false);
     build_adjoint(true);
@@ -705,7 +719,7 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
 bool Plan::tma_source(int l, const dev::StageArgs& A, TmaSource* out) const {
   const Layout& L = layouts_[l];
   const std::size_t D = L.gext.size();
-  if (!layout_separable(L) || A.n > 1024) return false;
+  if (!layout_even(L) || A.n > 1024) return false;
   const auto blocks = layout_blocks(L);
   const RankBlock& b0 = blocks.at(0);
   const std::size_t a = static_cast<std::size_t>(A.a), b = static_cast<std::size_t>(A.b);
@@ -1150,8 +1164,14 @@ void Plan::finalize_program(std::vector<Op>& prog, int cur_l, int cur_b, const L
 // Device resources
 // ---------------------------------------------------------------------------
 void Plan::allocate_device() {
-  // Scratch: the largest global array the programs hold.
+  // Scratch: the largest global array the programs hold (per-rank programs:
+  // the largest layout they use, so that the tuner's trial launches of the
+  // stages that read or write the exchange buffers fit).
   std::size_t max_elems = std::max(layout_elements(lin_), layout_elements(lout_));
+  if (is_rank_plan()) {
+    max_elems = 0;
+    for (const Layout& L : layouts_) max_elems = std::max(max_elems, layout_elements(L));
+  }
   const std::size_t scratch_bytes = max_elems * (d_.dbl ? 16 : 8);
   buf_bytes_.resize(std::max<std::size_t>(buf_bytes_.size(), kBufFirstDebug), 0);
   buf_bytes_[kBufScratch0] = scratch_bytes;
@@ -1382,16 +1402,19 @@ void Plan::autotune() {
 // ---------------------------------------------------------------------------
 // Execution
 // ---------------------------------------------------------------------------
-void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, cudaStream_t stream) const {
+void Plan::run_program(const std::vector<Op>& prog, const void* in, void* out, cudaStream_t stream,
+                       std::size_t begin, std::size_t end, void* send, void* recv) const {
   if (!on_device_) fail(kErrInvalidArgument, "plan was created by dfft_plan_analyze and cannot execute");
-  if (!in || !out) fail(kErrInvalidArgument, "null buffer");
-  if (in == out) fail(kErrInvalidArgument, "in-place execution is not supported: in and out must differ");
   auto buf = [&](int id) -> void* {
     if (id == kBufIn) return const_cast<void*>(in);
     if (id == kBufOut) return out;
+    if (id == kBufSend) return send;
+    if (id == kBufRecv) return recv;
     return bufs_.at(id);
   };
-  for (const Op& op0 : prog) {
+  end = std::min(end, prog.size());
+  for (std::size_t oi = begin; oi < end; ++oi) {
+    const Op& op0 = prog[oi];
     cudaError_t e = cudaSuccess;
     switch (op0.type) {
       case Op::Stage: {
@@ -1478,11 +1501,16 @@ void Plan::check_buffers(const void* in, const void* out, bool forward) const {
 }
 
 void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream) const {
+  if (is_rank_plan())
+    fail(kErrInvalidArgument, "a per-rank plan executes segment by segment around the caller's exchanges");
   check_buffers(in, out, forward);
   run_program(prog_[forward ? 0 : 1], in, out, stream);
 }
 
 void Plan::execute_adjoint(const void* in, void* out, bool of_forward, cudaStream_t stream) const {
+  if (is_rank_plan()) fail(kErrInvalidArgument, "per-rank plans have no adjoint programs");
+  if (!in || !out) fail(kErrInvalidArgument, "null buffer");
+  if (in == out) fail(kErrInvalidArgument, "in-place execution is not supported: in and out must differ");
   // adjoint of forward: complex output layout -> input layout; of backward: the reverse
   check_alignment(in, of_forward ? true : lin_.complex, "input");
   check_alignment(out, of_forward ? lin_.complex : true, "output");

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "dev_types.h"
+#include "exchange.hpp"
 #include "layout.hpp"
 #include "plan_core.hpp"
 
@@ -26,10 +27,28 @@ struct PlanDesc {
   int norm = 0;       // 0 backward, 1 forward, 2 ortho, 3 none
   int exec_mode = 0;  // 0 fused, 1 literal, 2 literal with capture of every exchange
   cudaStream_t stream = nullptr;
+  // >= 0: the program of this one world rank (one process per GPU): its local
+  // blocks only, with the exchanges left to the caller's communicator
+  long long rank = -1;
 };
 
-// Buffer ids used by the device programs.
-enum : int { kBufIn = 0, kBufOut = 1, kBufScratch0 = 2, kBufScratch1 = 3, kBufFirstDebug = 4 };
+// Buffer ids used by the device programs (send / recv: the caller's exchange
+// buffers of a per-rank program).
+enum : int { kBufRecv = -3, kBufSend = -2, kBufIn = 0, kBufOut = 1, kBufScratch0 = 2, kBufScratch1 = 3,
+             kBufFirstDebug = 4 };
+
+// One all-to-all of a per-rank program: the send buffer (the reference's
+// [group size, buffer extents] pack buffer of transpose block `block`) goes
+// out in equal chunks, one per group member, and the recv buffer of the same
+// size comes back.
+struct Exchange {
+  std::size_t block = 0;
+  int comm_axis = -1;  // -1 whole communicator; 0 / 1 row / column communicator
+  std::size_t elements = 0;
+  std::size_t elem_bytes = 0;
+  bool padded = false;  // the send buffer has entries past the bins that must stay zero
+  ExchangeGroup group;  // this rank's group (world ranks by sub-rank)
+};
 
 // Tiled tensor-map description of a TMA-fed stage's source layout (5
 // dimensions, unused ones of extent 1): byte strides of dimensions 1..4, the
@@ -132,6 +151,19 @@ class Plan {
   // block `block` to host: which = 0 send, 1 recv, 2 pack input, 3 unpack output.
   void export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const;
 
+  // Per-rank programs (desc().rank >= 0, rank.cpp).  A direction runs as
+  // segments: segment 0 reads `in`, every segment but the last ends by
+  // writing exchange k's send buffer, the caller's all-to-all fills its recv
+  // buffer, which segment k + 1 reads; the last segment writes `out`.
+  bool is_rank_plan() const { return d_.rank >= 0; }
+  const std::vector<Exchange>& exchanges(bool forward) const { return xch_[forward ? 0 : 1]; }
+  // Exchange group of any world rank for exchange k of a direction.
+  ExchangeGroup exchange_group_of(bool forward, std::size_t k, std::size_t rank) const;
+  void execute_segment(bool forward, std::size_t segment, const void* in, void* out, void* send, void* recv,
+                       cudaStream_t stream) const;
+  // Local extents (logical order) of this rank's input (which 0) / output (1) block.
+  Ext rank_local_extents(int which) const;
+
  private:
   PlanDesc d_;
   bool on_device_;
@@ -173,12 +205,21 @@ class Plan {
   void build_fused(bool forward);
   void build_literal(bool forward);
   void build_adjoint(bool of_forward);
-  void run_program(const std::vector<Op>& prog, const void* in, void* out, cudaStream_t stream) const;
+  void run_program(const std::vector<Op>& prog, const void* in, void* out, cudaStream_t stream,
+                   std::size_t begin = 0, std::size_t end = ~std::size_t(0), void* send = nullptr,
+                   void* recv = nullptr) const;
   void check_alignment(const void* p, bool complex, const char* which) const;
   void finalize_program(std::vector<Op>& prog, int cur_layout, int cur_buf, const Layout& final_layout,
                         double scale, bool final_complex);
   void allocate_device();
   void autotune();
+  // per-rank programs
+  std::vector<Exchange> xch_[2];
+  std::vector<std::size_t> seg_end_[2];  // op index one past each segment's last op
+  Layout rank_layout(std::size_t chain_index, bool complex) const;
+  Layout rank_buffer_layout(std::size_t chain_index, bool complex, std::size_t split_axis, const BlockInfo& b) const;
+  void rank_exchanges(bool forward);
+  void build_rank(bool forward);
   bool tma_source(int layout, const dev::StageArgs& A, TmaSource* out) const;
   cudaError_t launch_stage(const Op& op, dev::StageArgs A, cudaStream_t stream) const;
   const void* twiddle(std::size_t n);

@@ -4,6 +4,7 @@ Python mirror of the reference's ``KokkosFFT::Distributed`` plan interface on
 top of the C ABI of ``libdfft.so`` (include/dfft.h)."""
 from ._lib import LIB_PATH, lib  # noqa: F401  (loads libdfft.so or raises)
 from . import exchange  # noqa: F401
+from .distributed import DistributedPlan  # noqa: F401
 from .navier_stokes import NavierStokes, step_graph  # noqa: F401
 from .plan import (  # noqa: F401
     Batch,

@@ -70,6 +70,22 @@ class TransBlockDesc(ctypes.Structure):
     ]
 
 
+class ExchangeInfo(ctypes.Structure):
+    _fields_ = [
+        ("block", ctypes.c_int64),
+        ("comm_axis", ctypes.c_int32),
+        ("padded", ctypes.c_int32),
+        ("elements", ctypes.c_uint64),
+        ("element_bytes", ctypes.c_uint64),
+        ("group_size", ctypes.c_int64),
+    ]
+
+
+# int32_t (*)(void* user, int64_t k, const void* send, void* recv, uint64_t bytes_per_peer, void* stream)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_uint64, ctypes.c_void_p)
+
+
 class NsDiag(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("enstrophy", ctypes.c_double), ("divergence_l2", ctypes.c_double)]
 
@@ -85,6 +101,22 @@ SIGNATURES = {
     "dfft_plan_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PlanDesc)]),
     "dfft_plan_analyze": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PlanDesc)]),
     "dfft_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dfft_plan_create_rank": (
+        ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PlanDesc), ctypes.c_int64]),
+    "dfft_plan_analyze_rank": (
+        ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PlanDesc), ctypes.c_int64]),
+    "dfft_get_num_exchanges": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_get_exchange_info": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ExchangeInfo)]),
+    "dfft_get_exchange_group": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                       ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    "dfft_execute_segment": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "dfft_execute_exchanged": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                       ctypes.c_void_p, EXCHANGE_FN, ctypes.c_void_p, ctypes.c_void_p]),
     "dfft_execute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
     "dfft_execute_on_stream": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),

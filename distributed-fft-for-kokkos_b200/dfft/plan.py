@@ -97,11 +97,14 @@ class Plan:
       exec_mode : "fused" (default) or "literal" (reference block sequence)
       stream : CUDA stream handle (int) the plan launches on
       analyze_only : plan on the host only (no device memory; cannot execute)
+      process_rank : build only this world rank's program (one process per
+                     GPU; executed by dfft.DistributedPlan segment by segment)
     """
 
     def __init__(self, in_extents, out_extents, axes, in_topology, out_topology, real_input=False,
                  precision="float64", norm=Normalization.backward, layout="right", in_topology_layout="right",
-                 out_topology_layout="right", exec_mode="fused", stream=None, analyze_only=False):
+                 out_topology_layout="right", exec_mode="fused", stream=None, analyze_only=False,
+                 process_rank=None):
         rank = len(in_extents)
         if not (len(out_extents) == len(in_topology) == len(out_topology) == rank):
             raise DistributedFFTError(Status.INVALID_ARGUMENT, "extents and topologies must have the view rank")
@@ -142,8 +145,13 @@ class Plan:
         self.out_topology = tuple(int(x) for x in out_topology)
         self.layout = layout
         self._h = ctypes.c_void_p()
-        fn = lib.dfft_plan_analyze if analyze_only else lib.dfft_plan_create
-        _check(fn(ctypes.byref(self._h), ctypes.byref(d)))
+        self.process_rank = None if process_rank is None else int(process_rank)
+        if process_rank is None:
+            fn = lib.dfft_plan_analyze if analyze_only else lib.dfft_plan_create
+            _check(fn(ctypes.byref(self._h), ctypes.byref(d)))
+        else:
+            fn = lib.dfft_plan_analyze_rank if analyze_only else lib.dfft_plan_create_rank
+            _check(fn(ctypes.byref(self._h), ctypes.byref(d), int(process_rank)))
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -190,6 +190,69 @@ dfft_status dfft_get_max_buffer_size(const dfft_plan* plan, uint64_t* size);
 dfft_status dfft_get_topology_chain(const dfft_plan* plan, int64_t* n, uint64_t* topologies, int64_t* trans_axes,
                                     int64_t* layouts);
 
+/* ---- One process per GPU: per-rank plans ----
+ * The reference's distributed Plan on one MPI / NCCL rank
+ * (KokkosFFT_Distributed_Plan.hpp:154-238 with a communicator of
+ * nprocs = prod(in_topology) ranks): the plan holds only rank `rank`'s
+ * program, reads its local input block and writes its local output block
+ * (dfft_get_local_extents with that rank, logical axis order, contiguous in
+ * the view's memory order), and leaves every all-to-all of a TransBlock
+ * (KokkosFFT_Distributed_TransBlock.hpp:76-107) to the caller's communicator,
+ * as the reference's backends do with MPI_Alltoall or ncclSend / ncclRecv
+ * pairs (KokkosFFT_Distributed_MPI_All2All.hpp:23-58,
+ * KokkosFFT_Distributed_NCCL_All2All.hpp:21-89).
+ *
+ * A direction runs as dfft_get_num_exchanges + 1 segments.  Segment 0 reads
+ * `in`; every segment but the last ends with exchange k's send buffer
+ * written in the reference's pack order ([group size, buffer extents] for
+ * LayoutRight views, [buffer extents, group size] for LayoutLeft: the pack
+ * folded into the last FFT stage's stores); the caller's all-to-all over the
+ * exchange's group then sends chunk j (element_bytes * elements / group_size
+ * bytes) to group member j and receives chunk j from member j; segment k + 1
+ * reads the recv buffer in place (the unpack folded into the next stage's
+ * loads); the last segment writes `out`.  The group of exchange k is the
+ * whole communicator (slab plans) or the row / column communicator of the
+ * Cartesian grid over the split entries of in_topology
+ * (KokkosFFT_Distributed_PencilPlan.hpp:32-71), members in rank order.  When
+ * `padded` is set, entries of the send buffer past the pack bins are never
+ * written: keep them zero (clear the buffer once) so that the exchanged bytes
+ * equal the reference's. */
+dfft_status dfft_plan_create_rank(dfft_plan** plan, const dfft_plan_desc* desc, int64_t rank);
+/* Host-only form (queries only). */
+dfft_status dfft_plan_analyze_rank(dfft_plan** plan, const dfft_plan_desc* desc, int64_t rank);
+
+typedef struct {
+  int64_t block;          /* index of the transpose block in the block list */
+  int32_t comm_axis;      /* -1 whole communicator, 0 row, 1 column communicator */
+  int32_t padded;         /* 1: the send buffer has entries no segment writes (keep them zero) */
+  uint64_t elements;      /* elements of the send buffer (= recv buffer), all peers' chunks */
+  uint64_t element_bytes; /* bytes of one element (real before the first R2C stage, complex after) */
+  int64_t group_size;     /* members of the exchange group (chunks of the buffers) */
+} dfft_exchange_info;
+
+dfft_status dfft_get_num_exchanges(const dfft_plan* plan, int32_t direction, int64_t* n);
+dfft_status dfft_get_exchange_info(const dfft_plan* plan, int32_t direction, int64_t k, dfft_exchange_info* info);
+/* Group of exchange k as seen by world rank `rank` (any rank, so that every
+ * process can create every sub-communicator collectively): its index in the
+ * group and the group's world ranks by group index (group_size entries). */
+dfft_status dfft_get_exchange_group(const dfft_plan* plan, int32_t direction, int64_t k, int64_t rank,
+                                    int64_t* sub_rank, int64_t* members);
+/* Run one segment on `stream`.  in: segment 0; out: the last segment; send:
+ * every segment but the last (exchange `segment`'s send buffer); recv: every
+ * segment but the first (exchange `segment - 1`'s recv buffer). */
+dfft_status dfft_execute_segment(const dfft_plan* plan, int32_t direction, int64_t segment, const void* in,
+                                 void* out, void* send, void* recv, void* stream);
+
+/* All segments of a direction with the caller's all-to-all in between:
+ * exchange(user, k, send, recv, bytes_per_peer, stream) must move exchange
+ * k's chunks (ordered on `stream`, or complete before returning) and return
+ * 0, or non-zero to abort (DFFT_ERROR_CUDA with that code in the message).
+ * send and recv must hold the largest exchange. */
+typedef int32_t (*dfft_exchange_fn)(void* user, int64_t k, const void* send, void* recv, uint64_t bytes_per_peer,
+                                    void* stream);
+dfft_status dfft_execute_exchanged(const dfft_plan* plan, const void* in, void* out, int32_t direction, void* send,
+                                   void* recv, dfft_exchange_fn exchange, void* user, void* stream);
+
 /* ---- Batched execution under a CUDA graph ----
  * Captures, once, the execution of `count` transforms (plans[i] applied to
  * ins[i] -> outs[i] in directions[i]) into one CUDA graph.  Transforms with

@@ -44,6 +44,10 @@ struct StageArgs {
   // off_a[p] = abase + p * astride (checked on the host), so positions along
   // the line are addressed without a table read
   int64_t src_abase, dst_abase, src_astride, dst_astride;
+  // register kernels, general-layout variant: 1 = a separable side whose
+  // offsets along a are not affine (an exchange buffer split into bins along
+  // a): positions along the line are read from the axis table (abase = 0)
+  int src_atab, dst_atab;
   // register kernels, separable sides: start of the offset tables of axes a,
   // b, o0, o1 in src.t / dst.t (filled by the launcher from src.off /
   // dst.off, so the kernels select no table at run time)

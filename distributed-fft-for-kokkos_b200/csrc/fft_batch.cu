@@ -53,7 +53,7 @@ cudaError_t launch_fft_batch(BatchParams& P, bool dbl, int kind, bool inverse, b
   // separable sides on every field: the variant without the general-layout
   // addressing (fewer registers)
   bool general = false;
-  for (int i = 0; i < P.nfields; ++i) general = general || P.f[i].src_line_affine || P.f[i].dst_line_affine;
+  for (int i = 0; i < P.nfields; ++i) general = general || P.f[i].src_line_affine || P.f[i].dst_line_affine || P.f[i].src_atab || P.f[i].dst_atab;
   return general ? launch_batch_variant<true>(P, dbl, kind, inverse, afast, st)
                  : launch_batch_variant<false>(P, dbl, kind, inverse, afast, st);
 }

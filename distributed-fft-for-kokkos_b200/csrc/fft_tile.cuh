@@ -86,10 +86,17 @@ __device__ __forceinline__ void fast_tile(const StageArgs& A, int tb, int co0, i
         stride = A.src_astride;
       }
       const C* row = in + base;
+      if (A.src_atab) {
 #pragma unroll
-      for (int q = 0; q < Q0; ++q)
+        for (int q = 0; q < Q0; ++q)
 #pragma unroll
-        for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r) * stride];
+          for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[__ldg(ls.t + A.s_ta + in_pos<N, 0, TT>(t, q, r))];
+      } else {
+#pragma unroll
+        for (int q = 0; q < Q0; ++q)
+#pragma unroll
+          for (int r = 0; r < R0; ++r) v[q * R0 + r] = row[in_pos<N, 0, TT>(t, q, r) * stride];
+      }
     } else if (AFAST) {
       const C* row = in + so + __ldg(ls.t + A.s_tb + b0 + line) + A.src_abase;
 #pragma unroll
@@ -138,10 +145,17 @@ __device__ __forceinline__ void fast_tile(const StageArgs& A, int tb, int co0, i
         stride = A.dst_astride;
       }
       C* row = out + base;
+      if (A.dst_atab) {
 #pragma unroll
-      for (int q = 0; q < QL; ++q)
+        for (int q = 0; q < QL; ++q)
 #pragma unroll
-        for (int r = 0; r < RL; ++r) row[(t + last_rel<N, TT>(q, r)) * stride] = v[q * RL + r];
+          for (int r = 0; r < RL; ++r) row[__ldg(ld.t + A.d_ta + t + last_rel<N, TT>(q, r))] = v[q * RL + r];
+      } else {
+#pragma unroll
+        for (int q = 0; q < QL; ++q)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) row[(t + last_rel<N, TT>(q, r)) * stride] = v[q * RL + r];
+      }
     } else if (AFAST) {
       C* row = out + dof + __ldg(ld.t + A.d_tb + b0 + line) + A.dst_abase;
 #pragma unroll
@@ -226,6 +240,11 @@ __device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, i
     drow1 = dof + (act1 ? __ldg(ld.t + A.d_tb + b0 + r1) : 0);
   }
   const T s = T(A.scale);
+  // position p of a line -> offset from its row base: p, or (general-layout
+  // variant, a side split into bins along a) the axis table
+  const bool satab = AFF && A.src_atab, datab = AFF && A.dst_atab;
+  auto spos = [&](int p) -> int64_t { return satab ? __ldg(ls.t + A.s_ta + p) : p; };
+  auto dpos = [&](int p) -> int64_t { return datab ? __ldg(ld.t + A.d_ta + p) : p; };
 
   C v[V];
   constexpr int R0 = Radix<N, 0>::value, Q0 = V / R0;
@@ -237,7 +256,7 @@ __device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, i
     for (int q = 0; q < Q0; ++q)
 #pragma unroll
       for (int r = 0; r < R0; ++r) {
-        const int p = in_pos<N, 0, TT>(t, q, r);
+        const int64_t p = spos(in_pos<N, 0, TT>(t, q, r));
         v[q * R0 + r] = mk<T>(act0 ? row0[p] : T(0), act1 ? row1[p] : T(0));
       }
     __syncthreads();  // twiddles staged
@@ -246,8 +265,9 @@ __device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, i
     const C* row0 = in + srow0;
     const C* row1 = in + srow1;
     for (int k = t; k <= H; k += TT) {
-      const C x0 = act0 ? row0[k] : mk<T>(T(0), T(0));
-      const C x1 = act1 ? row1[k] : mk<T>(T(0), T(0));
+      const int64_t pk = spos(k);
+      const C x0 = act0 ? row0[pk] : mk<T>(T(0), T(0));
+      const C x1 = act1 ? row1[pk] : mk<T>(T(0), T(0));
       if (k == 0 || k == H) {
         ln[padpos<S>(k)] = mk<T>(x0.x, x1.x);
       } else {
@@ -280,10 +300,11 @@ __device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, i
     for (int k = t; k <= H; k += TT) {
       const C z = ln[padpos<S>(k)];
       const C zc = cconj(ln[padpos<S>(k == 0 ? 0 : N - k)]);
-      if (act0) row0[k] = cscale(cadd(z, zc), hs);
+      const int64_t pk = dpos(k);
+      if (act0) row0[pk] = cscale(cadd(z, zc), hs);
       if (act1) {
         const C d = csub(z, zc);
-        row1[k] = mk<T>(d.y * hs, -d.x * hs);
+        row1[pk] = mk<T>(d.y * hs, -d.x * hs);
       }
     }
   } else {
@@ -294,7 +315,7 @@ __device__ __forceinline__ void real_tile(const StageArgs& A, int tb, int co0, i
     for (int q = 0; q < QL; ++q)
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
-        const int p = t + last_rel<N, TT>(q, r);
+        const int64_t p = dpos(t + last_rel<N, TT>(q, r));
         if (act0) row0[p] = v[q * RL + r].x * s;
         if (act1) row1[p] = v[q * RL + r].y * s;
       }

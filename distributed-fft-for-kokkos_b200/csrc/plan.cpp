@@ -606,23 +606,35 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   // contiguous run) or general tables whose rank blocks do not split axis a
   // (every line is affine, base + p * stride; lines read along a have unit
   // stride because a is the layout's fast axis).
-  auto side_ok = [&](int l, const Layout& L, std::size_t len, bool afast, int* affine, std::int64_t* abase,
-                     std::int64_t* astride) {
+  auto side_ok = [&](int l, const Layout& L, std::size_t len, bool afast, int* affine, int* atab,
+                     std::int64_t* abase, std::int64_t* astride) {
     const LayoutTables& T = tables_[l];
+    *atab = 0;
     if (T.mode == 0) {
       // separable: the offsets along a must be affine (unit stride when the
       // lines are read along a)
       *affine = 0;
       const std::int64_t* off = T.data.data() + T.off[a];
       const std::int64_t st = len > 1 ? off[1] - off[0] : 1;
-      if (afast && st != 1) return false;
-      for (std::size_t c = 1; c < len; ++c)
-        if (off[c] != off[0] + static_cast<std::int64_t>(c) * st) return false;
+      bool aff = !afast || st == 1;
+      for (std::size_t c = 1; aff && c < len; ++c)
+        if (off[c] != off[0] + static_cast<std::int64_t>(c) * st) aff = false;
       // the kernels take 32-bit offsets along a line
-      if (static_cast<std::int64_t>(len - 1) * (st < 0 ? -st : st) >= (std::int64_t(1) << 31)) return false;
-      *abase = off[0];
-      *astride = st;
-      return true;
+      if (aff && static_cast<std::int64_t>(len - 1) * (st < 0 ? -st : st) >= (std::int64_t(1) << 31)) aff = false;
+      if (aff) {
+        *abase = off[0];
+        *astride = st;
+        return true;
+      }
+      // an exchange buffer split into bins along a (per-rank programs): the
+      // general-layout kernel variant reads positions from the axis table
+      if (!L.pad.empty() && L.topo[a] > 1 && (!afast || layout_fast_axis(L) == a)) {
+        *atab = 1;
+        *abase = 0;
+        *astride = 1;
+        return true;
+      }
+      return false;
     }
     *affine = 1;
     return L.topo[a] == 1 && (!afast || layout_fast_axis(L) == a);
@@ -633,12 +645,12 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   const std::size_t Bf = (grid_ok && dev::fast_stage_supported(static_cast<int>(n)))
                              ? static_cast<std::size_t>(dev::fast_stage_lines(d_.dbl, static_cast<int>(n)))
                              : 0;
-  int saff = 0, daff = 0;
+  int saff = 0, daff = 0, satab = 0, datab = 0;
   std::int64_t sab = 0, sas = 0, dab = 0, das = 0;
   // C2C: lines of n points on both sides, the same row orientation
   if (kind == dev::kC2C && Bf && A.load_afast == A.store_afast && S.gext[a] == n && Dl.gext[a] == n &&
-      side_ok(src_l, S, n, A.load_afast != 0, &saff, &sab, &sas) &&
-      side_ok(dst_l, Dl, n, A.load_afast != 0, &daff, &dab, &das)) {
+      side_ok(src_l, S, n, A.load_afast != 0, &saff, &satab, &sab, &sas) &&
+      side_ok(dst_l, Dl, n, A.load_afast != 0, &daff, &datab, &dab, &das)) {
     op.fast = true;
     A.B = static_cast<int>(Bf);
     A.tiles_b = static_cast<int>((Dl.gext[b] + Bf - 1) / Bf);
@@ -648,8 +660,8 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   const std::size_t nr = n, nc = n / 2 + 1;
   const std::size_t ns = kind == dev::kR2C ? nr : nc, ndst = kind == dev::kR2C ? nc : nr;
   if ((kind == dev::kR2C || kind == dev::kC2R) && Bf && A.load_afast && A.store_afast && S.gext[a] == ns &&
-      Dl.gext[a] == ndst && side_ok(src_l, S, ns, true, &saff, &sab, &sas) &&
-      side_ok(dst_l, Dl, ndst, true, &daff, &dab, &das)) {
+      Dl.gext[a] == ndst && side_ok(src_l, S, ns, true, &saff, &satab, &sab, &sas) &&
+      side_ok(dst_l, Dl, ndst, true, &daff, &datab, &dab, &das)) {
     op.fast = true;
     A.B = static_cast<int>(Bf);
     A.tiles_b = static_cast<int>((Dl.gext[b] + 2 * Bf - 1) / (2 * Bf));
@@ -657,6 +669,8 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
   if (op.fast) {
     A.src_line_affine = saff;
     A.dst_line_affine = daff;
+    A.src_atab = satab;
+    A.dst_atab = datab;
     A.src_abase = sab;
     A.src_astride = sas;
     A.dst_abase = dab;
@@ -680,6 +694,7 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
       return true;
     };
     if (kind == dev::kC2C && !d_.dbl && dev::pair_stage_supported(static_cast<int>(n)) && !saff && !daff &&
+        !satab && !datab &&
         (A.load_afast || (pair_aligned(src_l, sab, sas) && pair_aligned(dst_l, dab, das)))) {
       int opts[3];
       dev::pair_stage_line_options(static_cast<int>(n), A.load_afast != 0, opts);
@@ -1284,7 +1299,8 @@ void Plan::autotune() {
     for (auto& op : *progs) {
       if (op.type != Op::Stage || !op.fast) continue;
       dev::StageArgs& A = op.sa;
-      if (A.src_line_affine || A.dst_line_affine) continue;  // general layouts keep the default tile
+      if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab)
+        continue;  // general-layout variant: default tile only
       // Trial buffers: the op's own plan-owned buffers, else the scratch
       // pair; each must hold the whole layout the stage reads / writes
       // (chirp-z stages run their FFTs on arrays larger than the scratch).

@@ -34,10 +34,16 @@ def _rank_plans(case, precision):
     return full, [dfft.Plan(**kw, precision=precision, process_rank=r) for r in range(full.nprocs)]
 
 
-def _run(case, precision="float64"):
+def _run(case, precision="float64", stages=None):
+    """stages: expected launches per direction of every rank's program (the
+    FFT stages alone: pack and unpack folded into their stores and loads)."""
     import torch
     full, plans = _rank_plans(case, precision)
     P = full.nprocs
+    if stages is not None:
+        for p in plans:
+            assert p.launch_count(dfft.Direction.forward) == stages
+            assert p.launch_count(dfft.Direction.backward) == stages
     order = "C" if case["layout"] == "right" else "F"
     x = case_input(case, case["seed"])
     rdt = np.float64 if precision == "float64" else np.float32
@@ -99,13 +105,13 @@ def test_rank_programs_small(case):
     _case((3, 32, 24, 20), (1, 2, 3), (1, 2, 2, 1), (1, 1, 2, 2), True),
 ])
 def test_rank_programs_medium(case, precision):
-    _run(case, precision)
+    _run(case, precision, stages=len(case["axes"]) if case["in_extents"] == (64, 64, 64) else None)
 
 
 def test_rank_programs_256cubed_pencil_fp32():
     # the headline pencil at 256^3 on 16 per-rank programs: register / TMA
     # stages on the exchange buffers
-    _run(_case((256, 256, 256), (0, 1, 2), (4, 4, 1), (1, 4, 4), False, seed=1), "float32")
+    _run(_case((256, 256, 256), (0, 1, 2), (4, 4, 1), (1, 4, 4), False, seed=1), "float32", stages=3)
 
 
 def test_distributed_plan_two_processes_on_one_gpu(tmp_path):

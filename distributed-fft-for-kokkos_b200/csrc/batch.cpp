@@ -20,9 +20,12 @@ bool batchable(const Op& op) {
   return dev::batch_stage_supported(op.sa.n);
 }
 
-// kind, inverse, a-fast rows, value class (3 * 2^k lengths or powers of two):
-// one batched launch per group
-using GroupKey = std::tuple<int, bool, bool, bool>;
+// kind, inverse, a-fast rows, line length: one batched launch per group
+using GroupKey = std::tuple<int, bool, bool, int>;
+
+void ck(cudaError_t e) {
+  if (e != cudaSuccess) fail(kErrCuda, std::string("batch stream fork / join: ") + cudaGetErrorString(e));
+}
 
 }  // namespace
 
@@ -44,6 +47,28 @@ Batch::Batch(std::vector<const Plan*> plans) : plans_(std::move(plans)) {
   dbl_ = plans_[0]->desc().dbl;
   for (const Plan* p : plans_)
     if (p->desc().dbl != dbl_) fail(kErrInvalidArgument, "all plans of a batch must have the same precision");
+  bool ok = cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; ok && i < kAux; ++i)
+    ok = cudaStreamCreateWithFlags(&aux_[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    release();
+    fail(kErrCuda, "batch stream / event creation failed");
+  }
+}
+
+Batch::~Batch() { release(); }
+
+void Batch::release() {
+  for (int i = 0; i < kAux; ++i) {
+    if (aux_[i]) cudaStreamDestroy(aux_[i]);
+    if (join_[i]) cudaEventDestroy(join_[i]);
+    aux_[i] = nullptr;
+    join_[i] = nullptr;
+  }
+  if (fork_) cudaEventDestroy(fork_);
+  fork_ = nullptr;
 }
 
 std::size_t Batch::launches(bool forward) const {
@@ -56,7 +81,7 @@ std::size_t Batch::launches(bool forward) const {
       if (s >= prog.size() || prog[s].tiles == 0) continue;
       const Op& op = prog[s];
       if (batchable(op))
-        ++groups[GroupKey(op.kind, op.inverse, op.sa.load_afast != 0, op.sa.n % 3 == 0)];
+        ++groups[GroupKey(op.kind, op.inverse, op.sa.load_afast != 0, op.sa.n)];
       else
         ++n;
     }
@@ -93,26 +118,52 @@ void Batch::execute(const void* const* ins, void* const* outs, bool forward, cud
       A.B = dev::batch_stage_lines(A.n);
       const int per = (op.kind == dev::kC2C) ? A.B : 2 * A.B;
       A.tiles_b = (A.Eb + per - 1) / per;
-      groups[GroupKey(op.kind, op.inverse, A.load_afast != 0, A.n % 3 == 0)].push_back(A);
+      groups[GroupKey(op.kind, op.inverse, A.load_afast != 0, A.n)].push_back(A);
     }
+    // one launch per group (and per kMaxBatchFields fields of it); within a
+    // launch the largest fields come first, so the last work items the
+    // persistent CTAs pick up are small tiles and the launch ends evenly
+    int nl = 0;
+    for (auto& g : groups) nl += static_cast<int>((g.second.size() + dev::kMaxBatchFields - 1) / dev::kMaxBatchFields);
+    fork(st, nl);
+    auto tiles_of = [](const dev::StageArgs& A) { return static_cast<long long>(A.tiles_b) * A.Eo0 * A.Eo1; };
+    int li = 0;
     for (auto& g : groups) {
-      const auto& list = g.second;
-      for (std::size_t c = 0; c < list.size(); c += dev::kMaxBatchFields) {
+      auto list = g.second;
+      std::stable_sort(list.begin(), list.end(),
+                       [&](const dev::StageArgs& x, const dev::StageArgs& y) { return tiles_of(x) > tiles_of(y); });
+      for (std::size_t c = 0; c < list.size(); c += dev::kMaxBatchFields, ++li) {
         dev::BatchParams P;
         std::memset(&P, 0, sizeof(P));
         P.nfields = static_cast<int>(std::min<std::size_t>(dev::kMaxBatchFields, list.size() - c));
         P.prefix[0] = 0;
         for (int i = 0; i < P.nfields; ++i) {
           P.f[i] = list[c + i];
-          const long long tiles = static_cast<long long>(P.f[i].tiles_b) * P.f[i].Eo0 * P.f[i].Eo1;
+          const long long tiles = tiles_of(P.f[i]);
           if (tiles >= (1ll << 31)) fail(kErrUnsupported, "too many tiles in one field of a batch");
           P.prefix[i + 1] = P.prefix[i] + tiles;
         }
+        const cudaStream_t ls = lane(st, li);
         const cudaError_t e = dev::launch_fft_batch(P, dbl_, std::get<0>(g.first), std::get<1>(g.first),
-                                                    std::get<2>(g.first), st);
+                                                    std::get<2>(g.first), ls);
         if (e != cudaSuccess) fail(kErrCuda, std::string("batched stage launch failed: ") + cudaGetErrorString(e));
       }
     }
+    join(st, nl);
+  }
+}
+
+void Batch::fork(cudaStream_t st, int lanes) const {
+  if (lanes <= 1) return;
+  ck(cudaEventRecord(fork_, st));
+  for (int i = 0; i < std::min(lanes - 1, kAux); ++i) ck(cudaStreamWaitEvent(aux_[i], fork_, 0));
+}
+
+void Batch::join(cudaStream_t st, int lanes) const {
+  if (lanes <= 1) return;
+  for (int i = 0; i < std::min(lanes - 1, kAux); ++i) {
+    ck(cudaEventRecord(join_[i], aux_[i]));
+    ck(cudaStreamWaitEvent(st, join_[i], 0));
   }
 }
 

@@ -62,6 +62,16 @@ struct StageArgs {
   // two-line kernels: 1 = last radix pass in compensated arithmetic (the
   // default tile of fft_pair_kernel and of the TMA kernel only)
   int comp;
+  // spectral pre-multiplier of the loaded values, general-layout variant of
+  // the one-line C2C kernel only (the first backward stage of a
+  // Navier-Stokes right-hand side on a 4D (3, nx, ny, nz / 2 + 1) spectrum):
+  // 0 none; 1 the 2/3-rule mask (keep |m_x| <= cut[0], |m_y| <= cut[1],
+  // m_z <= cut[2], signed modes m of axes 1 and 2, the half axis 3 has modes
+  // 0 .. n / 2); 2 + c: i k_c times the mask, k_c = m_c * kscale (c = 0, 1, 2)
+  int pre_mode;
+  int pre_n[2];    // extents of axes 1 and 2 (signed modes)
+  int pre_cut[3];  // cutoffs of axes 1, 2, 3
+  double pre_kscale;
 };
 
 // How the TMA-fed stage forms the 5 coordinates of a tile's box from the
@@ -140,8 +150,8 @@ cudaError_t launch_fft_pair_tma(const StageArgs& A, const void* map, const TmaCo
                                 cudaStream_t st);
 // Batched register stage (fft_batch.cu): one persistent launch runs the same
 // stage (kind, direction, row orientation) of up to kMaxBatchFields fields
-// whose line lengths share a value class (all powers of two, or all 3 * 2^k); field f owns work items prefix[f] .. prefix[f+1]
-// - 1, its tiles (tb + tiles_b (co0 + Eo0 co1)).  Every field's StageArgs
+// of one line length; field f owns work items prefix[f] .. prefix[f+1] - 1,
+// its tiles (tb + tiles_b (co0 + Eo0 co1)).  Every field's StageArgs
 // must have B = batch_stage_lines(n) (complex lines per tile) and the tiles_b
 // that goes with it; the args are taken by value (kernel parameter space).
 constexpr int kMaxBatchFields = 48;

@@ -1,16 +1,15 @@
 // Batched register FFT stages (sm_100a): one persistent launch runs one stage
-// of many fields of uneven sizes.
+// of many fields of uneven sizes that share the stage's line length.
 //
 // A CTA of kBatchThreads threads walks work items blockIdx.x, +gridDim.x, ...
 // of a table that concatenates the tiles of every field; for each item it
 // finds the field (the item index only grows, so the field index only
 // advances), decodes the tile (tb, co0, co1) of that field's stage and runs
-// the tile body of the stage's line length with B = kBatchThreads / (N / V)
-// lines, the same bodies as the one-tile-per-CTA kernels (fft_tile.cuh).
-// The switch on the line length is uniform across the CTA.  Shared memory is
-// sized for the largest tile of the launch; the twiddles are restaged only
-// when the line length changes from one tile of the CTA to the next; a barrier
-// separates consecutive tiles.
+// the tile body of the line length with B = kBatchThreads / (N / V) lines,
+// the same bodies as the one-tile-per-CTA kernels (fft_tile.cuh), at the
+// register budget of those kernels.  The twiddles are staged once per CTA; a
+// barrier separates consecutive tiles.  The host launches the lengths of one
+// stage index concurrently (batch.cpp).
 #include "fft_batch.cuh"
 
 namespace dfft {

@@ -17,14 +17,18 @@ using namespace radix;
 
 constexpr int kBatchThreads = 256;
 
-// A launch covers the lengths of one value class VC (8 values a thread:
-// powers of two; 24: 3 * 2^k), so each kernel's register budget is its own
-// class's: resident CTAs per SM for complex64 4 (64 registers) for 8-value
-// tiles and 3 (85 registers, the budget of the one-tile 24-value kernels)
-// for 24-value tiles; for complex128 2 and 1.
-template <typename T, int VC>
+// A launch covers the fields of one line length N, so each kernel carries one
+// tile body at a register budget of its own: resident threads per SM for
+// 8-value bodies 1536 complex64 / 768 complex128, for 24-value bodies 512 /
+// 256 (one step below the one-tile kernels of fft_fast.cu, which leaves the
+// work-table loop its registers without spilling); the general-layout
+// 8-value variant keeps the compiler's choice.
+template <typename T, int N, bool AFAST, bool AFF>
 struct BatchMinBlocks {
-  static constexpr int value = sizeof(T) == 4 ? (VC == 8 ? 4 : 3) : (VC == 8 ? 2 : 1);
+  static constexpr bool v8 = Vals<N>::value == 8;
+  static constexpr int target = v8 ? (sizeof(T) == 4 ? 1536 : 768) : (sizeof(T) == 4 ? 512 : 256);
+  static constexpr int v = target / kBatchThreads;
+  static constexpr int value = (!(v8 && AFF) && v > 0) ? v : 1;
 };
 
 template <int N>
@@ -32,9 +36,8 @@ struct BatchLines {
   static constexpr int value = kBatchThreads / (N / Vals<N>::value);
 };
 
-#define DFFT_BATCH_LENGTHS8(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048)
-#define DFFT_BATCH_LENGTHS24(X) X(24) X(48) X(96) X(192) X(384) X(768)
-#define DFFT_BATCH_LENGTHS(X) DFFT_BATCH_LENGTHS8(X) DFFT_BATCH_LENGTHS24(X)
+#define DFFT_BATCH_LENGTHS(X) \
+  X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(24) X(48) X(96) X(192) X(384) X(768)
 
 // tile (tb, co0, co1) of a field's stage from its local work index (32-bit:
 // the host keeps every field's tile count below 2^31)
@@ -46,50 +49,38 @@ __device__ __forceinline__ void decode(const StageArgs& A, unsigned local, int* 
   *co1 = static_cast<int>(rest / static_cast<unsigned>(A.Eo0));
 }
 
-template <typename T, bool INV, bool AFAST, bool AFF, int VC>
-__global__ void __launch_bounds__(kBatchThreads, (BatchMinBlocks<T, VC>::value)) fft_batch_c2c_kernel(const __grid_constant__ BatchParams P) {
+template <typename T, bool INV, bool AFAST, bool AFF, int N>
+__global__ void __launch_bounds__(kBatchThreads, (BatchMinBlocks<T, N, AFAST, AFF>::value))
+    fft_batch_c2c_kernel(const __grid_constant__ BatchParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long long total = P.prefix[P.nfields];
-  int f = 0, cur_n = 0;
+  int f = 0;
+  bool first = true;  // the twiddles of N are staged by the CTA's first tile
   for (long long w = blockIdx.x; w < total; w += gridDim.x) {
     while (w >= P.prefix[f + 1]) ++f;
     const StageArgs& A = P.f[f];
     int tb, co0, co1;
     decode(A, static_cast<unsigned>(w - P.prefix[f]), &tb, &co0, &co1);
-    const bool stage_tw = A.n != cur_n;
-    cur_n = A.n;
-#define DFFT_TILE(N_) \
-  case N_: fast_tile<T, INV, N_, BatchLines<N_>::value, AFAST, AFF>(A, tb, co0, co1, smem_raw, stage_tw); break;
-    if constexpr (VC == 8) {
-      switch (A.n) { DFFT_BATCH_LENGTHS8(DFFT_TILE) default: break; }
-    } else {
-      switch (A.n) { DFFT_BATCH_LENGTHS24(DFFT_TILE) default: break; }
-    }
-#undef DFFT_TILE
-    __syncthreads();  // the next tile restages twiddles and lines
+    fast_tile<T, INV, N, BatchLines<N>::value, AFAST, AFF>(A, tb, co0, co1, smem_raw, first);
+    first = false;
+    __syncthreads();  // the next tile restages its lines
   }
 }
 
-template <typename T, bool C2R, bool AFF, int VC>
-__global__ void __launch_bounds__(kBatchThreads, (BatchMinBlocks<T, VC>::value)) fft_batch_real_kernel(const __grid_constant__ BatchParams P) {
+template <typename T, bool C2R, bool AFF, int N>
+__global__ void __launch_bounds__(kBatchThreads, (BatchMinBlocks<T, N, true, AFF>::value))
+    fft_batch_real_kernel(const __grid_constant__ BatchParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long long total = P.prefix[P.nfields];
-  int f = 0, cur_n = 0;
+  int f = 0;
+  bool first = true;
   for (long long w = blockIdx.x; w < total; w += gridDim.x) {
     while (w >= P.prefix[f + 1]) ++f;
     const StageArgs& A = P.f[f];
     int tb, co0, co1;
     decode(A, static_cast<unsigned>(w - P.prefix[f]), &tb, &co0, &co1);
-    const bool stage_tw = A.n != cur_n;
-    cur_n = A.n;
-#define DFFT_TILE(N_) \
-  case N_: real_tile<T, C2R, N_, BatchLines<N_>::value, AFF>(A, tb, co0, co1, smem_raw, stage_tw); break;
-    if constexpr (VC == 8) {
-      switch (A.n) { DFFT_BATCH_LENGTHS8(DFFT_TILE) default: break; }
-    } else {
-      switch (A.n) { DFFT_BATCH_LENGTHS24(DFFT_TILE) default: break; }
-    }
-#undef DFFT_TILE
+    real_tile<T, C2R, N, BatchLines<N>::value, AFF>(A, tb, co0, co1, smem_raw, first);
+    first = false;
     __syncthreads();
   }
 }
@@ -125,33 +116,37 @@ cudaError_t launch_persistent(K kernel, BatchParams& P, size_t smem, cudaStream_
   return cudaGetLastError();
 }
 
-template <typename T, bool AFF, int VC>
-cudaError_t launch_batch_vc(BatchParams& P, size_t smem, int kind, bool inverse, bool afast, cudaStream_t st) {
+template <typename T, bool AFF, int N>
+cudaError_t launch_batch_n(BatchParams& P, size_t smem, int kind, bool inverse, bool afast, cudaStream_t st) {
   if (kind == kC2C) {
     if (inverse)
-      return afast ? launch_persistent(fft_batch_c2c_kernel<T, true, true, AFF, VC>, P, smem, st)
-                   : launch_persistent(fft_batch_c2c_kernel<T, true, false, AFF, VC>, P, smem, st);
-    return afast ? launch_persistent(fft_batch_c2c_kernel<T, false, true, AFF, VC>, P, smem, st)
-                 : launch_persistent(fft_batch_c2c_kernel<T, false, false, AFF, VC>, P, smem, st);
+      return afast ? launch_persistent(fft_batch_c2c_kernel<T, true, true, AFF, N>, P, smem, st)
+                   : launch_persistent(fft_batch_c2c_kernel<T, true, false, AFF, N>, P, smem, st);
+    return afast ? launch_persistent(fft_batch_c2c_kernel<T, false, true, AFF, N>, P, smem, st)
+                 : launch_persistent(fft_batch_c2c_kernel<T, false, false, AFF, N>, P, smem, st);
   }
-  if (kind == kR2C) return launch_persistent(fft_batch_real_kernel<T, false, AFF, VC>, P, smem, st);
-  if (kind == kC2R) return launch_persistent(fft_batch_real_kernel<T, true, AFF, VC>, P, smem, st);
+  if (kind == kR2C) return launch_persistent(fft_batch_real_kernel<T, false, AFF, N>, P, smem, st);
+  if (kind == kC2R) return launch_persistent(fft_batch_real_kernel<T, true, AFF, N>, P, smem, st);
   return cudaErrorInvalidValue;
 }
 
-// every field of P has line lengths of one value class (the host groups them)
+// every field of P has the same line length (the host groups them)
 template <typename T, bool AFF>
 cudaError_t launch_batch_t(BatchParams& P, int kind, bool inverse, bool afast, cudaStream_t st) {
-  size_t smem = 0;
-  const bool v24 = P.f[0].n % 3 == 0;
+  const int n = P.f[0].n;
+  const size_t smem = tile_smem<T>(n, kind == kC2C ? afast : true);
+  if (smem == 0) return cudaErrorInvalidValue;
   for (int i = 0; i < P.nfields; ++i) {
-    const size_t b = tile_smem<T>(P.f[i].n, kind == kC2C ? afast : true);
-    if (b == 0 || (P.f[i].n % 3 == 0) != v24) return cudaErrorInvalidValue;
-    if (b > smem) smem = b;
+    if (P.f[i].n != n) return cudaErrorInvalidValue;
     P.f[i] = with_table_offsets(P.f[i]);
   }
-  return v24 ? launch_batch_vc<T, AFF, 24>(P, smem, kind, inverse, afast, st)
-             : launch_batch_vc<T, AFF, 8>(P, smem, kind, inverse, afast, st);
+  switch (n) {
+#define DFFT_LAUNCH(N_) \
+  case N_: return launch_batch_n<T, AFF, N_>(P, smem, kind, inverse, afast, st);
+    DFFT_BATCH_LENGTHS(DFFT_LAUNCH)
+#undef DFFT_LAUNCH
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // the launcher of one addressing variant (AFF: general-layout sides),

@@ -89,7 +89,7 @@ static cudaError_t launch_fast_n(const StageArgs& A, cudaStream_t st) {
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
-  if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab)  // general layouts: default tile only
+  if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab || A.pre_mode)  // general layouts: default tile only
     return A.B == B0 ? launch_fast_b<T, N, INV, AF, B0, true>(A, st) : cudaErrorInvalidValue;
   if (A.B == B0) return launch_fast_b<T, N, INV, AF, B0>(A, st);
   if (A.B == B1) return launch_fast_b<T, N, INV, AF, B1>(A, st);
@@ -121,7 +121,7 @@ static cudaError_t launch_real_n(const StageArgs& A, cudaStream_t st) {
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
-  if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab)
+  if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab || A.pre_mode)
     return A.B == B0 ? launch_real_b<T, N, C2R, B0, true>(A, st) : cudaErrorInvalidValue;
   if (A.B == B0) return launch_real_b<T, N, C2R, B0>(A, st);
   if (A.B == B1) return launch_real_b<T, N, C2R, B1>(A, st);

@@ -124,6 +124,38 @@ __device__ __forceinline__ void fast_tile(const StageArgs& A, int tb, int co0, i
 #pragma unroll
     for (int e = 0; e < V; ++e) v[e] = mk<T>(T(0), T(0));
   }
+  if constexpr (AFF) {
+    if (A.pre_mode && active) {
+      // global spatial coordinates of the line (axes 1..3 of the 4D view):
+      // the one along a varies with the position, the others are fixed
+      int fixed[3], along = -1;
+#pragma unroll
+      for (int k = 1; k <= 3; ++k) {
+        fixed[k - 1] = k == A.b ? b0 + line : k == A.o0 ? co0 : k == A.o1 ? co1 : 0;
+        if (k == A.a) along = k - 1;
+      }
+#pragma unroll
+      for (int q = 0; q < Q0; ++q)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+          const int p = in_pos<N, 0, TT>(t, q, r);
+          int m[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) m[k] = along == k ? p : fixed[k];
+#pragma unroll
+          for (int k = 0; k < 2; ++k) m[k] = 2 * m[k] < A.pre_n[k] ? m[k] : m[k] - A.pre_n[k];
+          const bool keep = abs(m[0]) <= A.pre_cut[0] && abs(m[1]) <= A.pre_cut[1] && m[2] <= A.pre_cut[2];
+          C x = v[q * R0 + r];
+          if (!keep) x = mk<T>(T(0), T(0));
+          if (A.pre_mode >= 2) {
+            const int c = A.pre_mode - 2;
+            const T kc = T((c == 0 ? m[0] : c == 1 ? m[1] : m[2]) * A.pre_kscale);
+            x = mk<T>(-kc * x.y, kc * x.x);  // i k_c x
+          }
+          v[q * R0 + r] = x;
+        }
+    }
+  }
   __syncthreads();  // twiddles staged
 
   run_fft<T, INV, N, 0, TT, SH::S>(v, t, tw, tile + line * LP);

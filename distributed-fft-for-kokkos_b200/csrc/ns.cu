@@ -12,6 +12,7 @@
 // buffers through the plan's layout tables, so the spectral operators see the
 // global wavenumber of each element whatever the topology.  The RK4 stage
 // update is fused into the combine / projection kernel.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +25,8 @@
 #include "batch.hpp"
 #include "layout.hpp"
 #include "ns.hpp"
+
+#include <algorithm>
 #include "plan.hpp"
 
 namespace dfft {
@@ -113,13 +116,15 @@ __global__ void ns_rhs_rk_kernel(const DevLayout L, cplx<T>* adv, cplx<T>* uk, c
     const double inv_ksq = (ix == 0 && iy == 0 && iz == 0) ? 0.0 : 1.0 / ksq;
     const T visc = T(-nu * ksq);
     int64_t o[3];
-    cplx<T> r[3];
+    cplx<T> r[3], um[3];
     off3(L, ix, iy, iz, o);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       cplx<T> a = adv[o[d]];
       if (!keep) a = mk<T>(T(0), T(0));
-      const cplx<T> u = uk[o[d]];
+      // the dealiased state (the 2/3 rule applied to uk, main.cpp:220-233)
+      um[d] = keep ? uk[o[d]] : mk<T>(T(0), T(0));
+      const cplx<T> u = um[d];
       r[d] = mk<T>(-a.x + visc * u.x, -a.y + visc * u.y);
     }
     const T ikk = T(inv_ksq);
@@ -133,7 +138,7 @@ __global__ void ns_rhs_rk_kernel(const DevLayout L, cplx<T>* adv, cplx<T>* uk, c
       const cplx<T> hf = mk<T>(f.x * hh, f.y * hh);
       const int64_t q = o[d];
       if (step == 0) {
-        const cplx<T> y = uk[q];
+        const cplx<T> y = um[d];
         y0[q] = y;
         k1[q] = hf;
         uk[q] = mk<T>(y.x + hf.x / T(2), y.y + hf.y / T(2));
@@ -149,6 +154,7 @@ __global__ void ns_rhs_rk_kernel(const DevLayout L, cplx<T>* adv, cplx<T>* uk, c
                       y0[q].y + (a.y + T(2) * b.y + T(2) * c.y + hf.y) / T(6));
       } else {
         adv[q] = f;  // step < 0: store the right-hand side itself
+        uk[q] = um[d];  // and leave uk dealiased, as the reference's right-hand side does
       }
     }
   }
@@ -604,11 +610,38 @@ static void ns_combine_phase(NsState* s, void* uk, void* adv, int step, cudaStre
   ck(cudaGetLastError(), "ns rhs");
 }
 
+// Backward transforms of the dealiased velocity and its three derivative
+// spectra.  When the plan's first backward stage is a register C2C stage, the
+// prep phase is folded into that stage's loads: each transform reads uk and
+// multiplies by the 2/3-rule mask (and i k_c), so neither the masked spectrum
+// nor the derivative spectra are written to memory (the combine phase applies
+// the mask to uk itself).
+static void ns_backward_phase(NsState* s, void* uk, cudaStream_t st) {
+  if (!s->plan->can_premultiply()) {
+    ns_prep_phase(s, uk, st);
+    s->plan->execute(uk, s->u, false, st);
+    for (int k = 0; k < 3; ++k) s->plan->execute(s->dk[k], s->du[k], false, st);
+    return;
+  }
+  dev::StageArgs pre;
+  std::memset(&pre, 0, sizeof(pre));
+  pre.pre_n[0] = s->g.nx;
+  pre.pre_n[1] = s->g.ny;
+  pre.pre_cut[0] = s->g.cx;
+  pre.pre_cut[1] = s->g.cy;
+  pre.pre_cut[2] = s->g.cz;
+  pre.pre_kscale = s->g.kscale;
+  pre.pre_mode = 1;
+  s->plan->execute_backward_premul(uk, s->u, pre, st);
+  for (int k = 0; k < 3; ++k) {
+    pre.pre_mode = 2 + k;
+    s->plan->execute_backward_premul(uk, s->du[k], pre, st);
+  }
+}
+
 // step in 0..3: RK4 stage; step = -1: only the right-hand side, into `out`
 static void ns_rhs_stage(NsState* s, void* uk, int step, void* out, cudaStream_t st) {
-  ns_prep_phase(s, uk, st);
-  s->plan->execute(uk, s->u, false, st);
-  for (int k = 0; k < 3; ++k) s->plan->execute(s->dk[k], s->du[k], false, st);
+  ns_backward_phase(s, uk, st);
   ns_advection_phase(s, st);
   void* adv = step < 0 ? out : s->adv;
   s->plan->execute(s->u, adv, true, st);
@@ -621,8 +654,28 @@ static void ns_rhs_stage(NsState* s, void* uk, int step, void* out, cudaStream_t
 void ns_batch_step(NsState* const* s, void* const* uks, int n, const Batch& batch, cudaStream_t st) {
   std::vector<const void*> ins(n);
   std::vector<void*> outs(n);
+  // the pointwise phases of different fields run concurrently on the batch's
+  // lanes, fields dealt to the least loaded lane, largest first
+  const int lanes = std::min(n, Batch::kAux + 1);
+  std::vector<int> lane_of(n, 0), order(n);
+  {
+    std::vector<double> load(lanes, 0.0);
+    for (int f = 0; f < n; ++f) order[f] = f;
+    auto size_of = [&](int f) { return static_cast<double>(s[f]->g.nx) * s[f]->g.ny * s[f]->g.nz; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return size_of(a) > size_of(b); });
+    for (int f : order) {
+      const int l = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+      lane_of[f] = l;
+      load[l] += size_of(f);
+    }
+  }
+  auto per_field = [&](auto&& phase) {
+    batch.fork(st, lanes);
+    for (int f : order) phase(f, batch.lane(st, lane_of[f]));
+    batch.join(st, lanes);
+  };
   for (int step = 0; step < 4; ++step) {
-    for (int f = 0; f < n; ++f) ns_prep_phase(s[f], uks[f], st);
+    per_field([&](int f, cudaStream_t ls) { ns_prep_phase(s[f], uks[f], ls); });
     for (int f = 0; f < n; ++f) {
       ins[f] = uks[f];
       outs[f] = s[f]->u;
@@ -635,13 +688,13 @@ void ns_batch_step(NsState* const* s, void* const* uks, int n, const Batch& batc
       }
       batch.execute(ins.data(), outs.data(), false, st);
     }
-    for (int f = 0; f < n; ++f) ns_advection_phase(s[f], st);
+    per_field([&](int f, cudaStream_t ls) { ns_advection_phase(s[f], ls); });
     for (int f = 0; f < n; ++f) {
       ins[f] = s[f]->u;
       outs[f] = s[f]->adv;
     }
     batch.execute(ins.data(), outs.data(), true, st);
-    for (int f = 0; f < n; ++f) ns_combine_phase(s[f], uks[f], s[f]->adv, step, st);
+    per_field([&](int f, cudaStream_t ls) { ns_combine_phase(s[f], uks[f], s[f]->adv, step, ls); });
   }
 }
 

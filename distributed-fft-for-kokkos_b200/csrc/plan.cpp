@@ -1523,6 +1523,37 @@ void Plan::execute(const void* in, void* out, bool forward, cudaStream_t stream)
   run_program(prog_[forward ? 0 : 1], in, out, stream);
 }
 
+bool Plan::can_premultiply() const {
+  if (is_rank_plan() || !on_device_ || prog_[1].empty()) return false;
+  const Op& op = prog_[1].front();
+  return op.type == Op::Stage && op.fast && op.kind == dev::kC2C && op.src == kBufIn &&
+         dev::fast_stage_supported(op.sa.n);
+}
+
+void Plan::execute_backward_premul(const void* in, void* out, const dev::StageArgs& pre, cudaStream_t stream) const {
+  if (!can_premultiply()) fail(kErrInternal, "the first backward stage cannot pre-multiply its loads");
+  check_buffers(in, out, false);
+  const auto& prog = prog_[1];
+  Op op = prog.front();
+  dev::StageArgs A = op.sa;
+  // the one-line kernel, general-layout variant, default tile
+  A.pairs = 0;
+  A.comp = 0;
+  A.B = dev::fast_stage_lines(d_.dbl, A.n);
+  A.tiles_b = (A.Eb + A.B - 1) / A.B;
+  op.tiles = static_cast<unsigned>(static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1);
+  A.pre_mode = pre.pre_mode;
+  A.pre_n[0] = pre.pre_n[0];
+  A.pre_n[1] = pre.pre_n[1];
+  for (int k = 0; k < 3; ++k) A.pre_cut[k] = pre.pre_cut[k];
+  A.pre_kscale = pre.pre_kscale;
+  A.in = const_cast<void*>(in);
+  A.out = op.dst == kBufOut ? out : bufs_.at(op.dst);
+  const cudaError_t e = launch_stage(op, A, stream);
+  if (e != cudaSuccess) fail(kErrCuda, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+  run_program(prog, in, out, stream, 1);
+}
+
 void Plan::execute_adjoint(const void* in, void* out, bool of_forward, cudaStream_t stream) const {
   if (is_rank_plan()) fail(kErrInvalidArgument, "per-rank plans have no adjoint programs");
   if (!in || !out) fail(kErrInvalidArgument, "null buffer");

@@ -151,6 +151,14 @@ class Plan {
   // block `block` to host: which = 0 send, 1 recv, 2 pack input, 3 unpack output.
   void export_buffers(bool forward, std::size_t block, int which, void* host, std::size_t capacity) const;
 
+  // Backward transform whose first stage multiplies every loaded value by a
+  // spectral factor (dev::StageArgs::pre_mode and the geometry in pre; the
+  // stage runs the general-layout one-line kernel).  can_premultiply(): the
+  // first backward stage is a register C2C stage, else the caller applies the
+  // factor itself.
+  bool can_premultiply() const;
+  void execute_backward_premul(const void* in, void* out, const dev::StageArgs& pre, cudaStream_t stream) const;
+
   // Per-rank programs (desc().rank >= 0, rank.cpp).  A direction runs as
   // segments: segment 0 reads `in`, every segment but the last ends by
   // writing exchange k's send buffer, the caller's all-to-all fills its recv

@@ -124,12 +124,18 @@ struct NsOf<N, 0> {
 // offline model of the bank wavefronts of every exchange of every plan and
 // thread mapping (one pad per 8 elements, or per 16 for complex64 lines of
 // 128+ points read along the line), which keeps the exchanges within ~1.1x of
-// conflict-free.
+// conflict-free.  Lines of 3 * 2^k points read along the line (a-fast: 8
+// threads of a line, 4 lines per warp) up to 192 points in complex64 and every
+// such length in complex128 take S = 3 and one more pad: with the general
+// rule their exchanges and the R2C / C2R half-spectrum passes ran at 2x the
+// conflict-free wavefronts (measured: 8M bank conflicts per 192-point R2C
+// launch of 340 MB), with this shape within 1.09x.
 template <typename T, int N, int B, bool AFAST>
 struct SmemShape {
   static constexpr bool f32 = sizeof(T) == 4;
-  static constexpr int S = (f32 && ((AFAST && N >= 128) || (!AFAST && B == 1))) ? 4 : 3;
-  static constexpr int extra_afast = (N <= (f32 ? 64 : 32)) ? 1 : 0;
+  static constexpr bool v24 = AFAST && N % 3 == 0 && !(f32 && N >= 384);
+  static constexpr int S = v24 ? 3 : (f32 && ((AFAST && N >= 128) || (!AFAST && B == 1))) ? 4 : 3;
+  static constexpr int extra_afast = (v24 || N <= (f32 ? 64 : 32)) ? 1 : 0;
   static constexpr int full = f32 ? 16 : 8;
   static constexpr int extra_bfast = (B >= full) ? 0 : (B * 2 == full) ? 3 : (B * 4 == full) ? 5 : (B * 8 == full) ? 9 : 0;
   static constexpr int LP = (N - 1) + ((N - 1) >> S) + 1 + (AFAST ? extra_afast : extra_bfast);

@@ -357,16 +357,26 @@ __device__ __forceinline__ void run_fft(cplx<T>* v, int t, const cplx<T>* tw, cp
 }
 
 // Base offset and stride along a of line (b = lb, o0 = c0, o1 = c1) of a
-// layout whose rank blocks do not split axis a.
+// general-layout side whose rank blocks do not split axis a: the line lies in
+// one rank block, found from the other coordinates (axis a contributes rank
+// 0 and local index 0 at position 0), and its stride is that block's stride
+// of axis a.
 __device__ __forceinline__ void line_affine(const DevLayout& L, const StageArgs& A, int lb, int c0, int c1,
                                             int64_t* base, int64_t* stride) {
   int c[4] = {0, 0, 0, 0};
   c[A.b] = lb;
   if (A.o0 >= 0) c[A.o0] = c0;
   if (A.o1 >= 0) c[A.o1] = c1;
-  *base = layout_offset(L, c, A.nd);
-  c[A.a] = 1;
-  *stride = layout_offset(L, c, A.nd) - *base;
+  int64_t r = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < A.nd && k != A.a) r += __ldg(L.t + L.rk[k] + c[k]);
+  int64_t o = __ldg(L.t + L.rbase + r);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < A.nd && k != A.a) o += __ldg(L.t + L.loc[k] + c[k]) * __ldg(L.t + L.rstride + r * 4 + k);
+  *base = o;
+  *stride = __ldg(L.t + L.rstride + r * 4 + A.a);
 }
 
 

@@ -41,19 +41,25 @@ struct NsGeom {
 
 __device__ __forceinline__ int signed_mode(int i, int n) { return (2 * i < n) ? i : i - n; }
 
-// offset of component d at global (ix, iy, iz) in a 4D layout
-__device__ __forceinline__ int64_t off4(const DevLayout& L, int d, int ix, int iy, int iz) {
-  int c[4] = {d, ix, iy, iz};
-  return layout_offset(L, c, 4);
-}
-
 // offsets of the 3 components at (ix, iy, iz): the component axis is not
-// split across ranks, so they are o(0) + d * (o(1) - o(0))
+// split across ranks, so they are o(0) + d * step, step the component stride
+// of the rank block that holds the point (one table walk for all three)
 __device__ __forceinline__ void off3(const DevLayout& L, int ix, int iy, int iz, int64_t* o) {
-  o[0] = off4(L, 0, ix, iy, iz);
-  const int64_t step = off4(L, 1, ix, iy, iz) - o[0];
-  o[1] = o[0] + step;
-  o[2] = o[1] + step;
+  int64_t base, step;
+  if (L.mode == 0) {
+    const int64_t c0 = __ldg(L.t + L.off[0]);
+    base = c0 + __ldg(L.t + L.off[1] + ix) + __ldg(L.t + L.off[2] + iy) + __ldg(L.t + L.off[3] + iz);
+    step = __ldg(L.t + L.off[0] + 1) - c0;
+  } else {
+    const int64_t r = __ldg(L.t + L.rk[1] + ix) + __ldg(L.t + L.rk[2] + iy) + __ldg(L.t + L.rk[3] + iz);
+    const int64_t* rs = L.t + L.rstride + r * 4;
+    base = __ldg(L.t + L.rbase + r) + __ldg(L.t + L.loc[1] + ix) * __ldg(rs + 1) +
+           __ldg(L.t + L.loc[2] + iy) * __ldg(rs + 2) + __ldg(L.t + L.loc[3] + iz) * __ldg(rs + 3);
+    step = __ldg(rs + 0);
+  }
+  o[0] = base;
+  o[1] = base + step;
+  o[2] = base + 2 * step;
 }
 
 template <typename T>

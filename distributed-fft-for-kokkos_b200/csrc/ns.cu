@@ -41,6 +41,22 @@ struct NsGeom {
 
 __device__ __forceinline__ int signed_mode(int i, int n) { return (2 * i < n) ? i : i - n; }
 
+// (ix, iy, iz) of point t of an (nx, ny, nz) box in C order; 32-bit unsigned
+// divisions whenever the index fits (every grid up to 1625^3)
+__device__ __forceinline__ void decode_point(int64_t t, int nz, int ny, int* ix, int* iy, int* iz) {
+  if (t < (int64_t(1) << 32)) {
+    const unsigned u = static_cast<unsigned>(t), q = u / static_cast<unsigned>(nz);
+    *iz = static_cast<int>(u - q * static_cast<unsigned>(nz));
+    *iy = static_cast<int>(q % static_cast<unsigned>(ny));
+    *ix = static_cast<int>(q / static_cast<unsigned>(ny));
+  } else {
+    const int64_t q = t / nz;
+    *iz = static_cast<int>(t - q * nz);
+    *iy = static_cast<int>(q % ny);
+    *ix = static_cast<int>(q / ny);
+  }
+}
+
 // offsets of the 3 components at (ix, iy, iz): the component axis is not
 // split across ranks, so they are o(0) + d * step, step the component stride
 // of the rank block that holds the point (one table walk for all three)
@@ -67,9 +83,8 @@ __global__ void ns_prep_kernel(const DevLayout L, cplx<T>* uk, cplx<T>* dx, cplx
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
     const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
     const T kx = T(mx * g.kscale), ky = T(my * g.kscale), kz = T(mz * g.kscale);
@@ -94,9 +109,8 @@ __global__ void ns_advection_kernel(const DevLayout L, T* u, const T* ux, const 
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nz;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nz);
-    const int iy = static_cast<int>((t / g.nz) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nz) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nz, g.ny, &ix, &iy, &iz);
     int64_t o[3];
     off3(L, ix, iy, iz, o);
     const T a = u[o[0]], b = u[o[1]], c = u[o[2]];
@@ -112,9 +126,8 @@ __global__ void ns_rhs_rk_kernel(const DevLayout L, cplx<T>* adv, cplx<T>* uk, c
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
     const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
     const double kx = mx * g.kscale, ky = my * g.kscale, kz = mz * g.kscale;
@@ -173,9 +186,8 @@ __global__ void ns_project_kernel(const DevLayout L, cplx<T>* uk, NsGeom g) {
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
     const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
     const double kx = mx * g.kscale, ky = my * g.kscale, kz = mz * g.kscale;
@@ -202,9 +214,8 @@ __global__ void ns_taylor_green_kernel(const DevLayout L, T* u, NsGeom g, double
   const double pi = 3.14159265358979323846;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nz);
-    const int iy = static_cast<int>((t / g.nz) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nz) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nz, g.ny, &ix, &iy, &iz);
     const double x = lx * pi * ix / g.nx, y = lx * pi * iy / g.ny, z = lx * pi * iz / g.nz;
     int64_t o[3];
     off3(L, ix, iy, iz, o);
@@ -225,9 +236,8 @@ __global__ void ns_energy_kernel(const DevLayout L, const cplx<T>* uk, NsGeom g,
   double acc = 0.0;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const double factor = (iz == 0) ? 1.0 : 2.0;
     double e = 0.0;
     int64_t o[3];
@@ -250,9 +260,8 @@ __global__ void ns_vorticity_kernel(const DevLayout L, const cplx<T>* uk, cplx<T
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const T kx = T(signed_mode(ix, g.nx) * g.kscale), ky = T(signed_mode(iy, g.ny) * g.kscale),
             kz = T(iz * g.kscale);
     int64_t o[3];
@@ -289,9 +298,8 @@ __global__ void ns_diag_kernel(const DevLayout L, const cplx<T>* uk, NsGeom g, d
   double ae = 0.0, aw = 0.0, ad = 0.0;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const double kx = signed_mode(ix, g.nx) * g.kscale, ky = signed_mode(iy, g.ny) * g.kscale, kz = iz * g.kscale;
     const double f = (iz == 0) ? 1.0 : 2.0;
     int64_t o[3];
@@ -353,9 +361,8 @@ __global__ void ns_dealias_kernel(const DevLayout L, const cplx<T>* src, cplx<T>
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const bool keep = abs(signed_mode(ix, g.nx)) <= g.cx && abs(signed_mode(iy, g.ny)) <= g.cy && iz <= g.cz;
     int64_t o[3];
     off3(L, ix, iy, iz, o);
@@ -370,9 +377,8 @@ __global__ void ns_adj_pre_kernel(const DevLayout L, const cplx<T>* c, cplx<T>* 
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
     const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
     const double kx = mx * g.kscale, ky = my * g.kscale, kz = mz * g.kscale;
@@ -402,9 +408,8 @@ __global__ void ns_adj_point_kernel(const DevLayout L, const T* u, T* d0, T* d1,
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nz;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nz);
-    const int iy = static_cast<int>((t / g.nz) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nz) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nz, g.ny, &ix, &iy, &iz);
     int64_t o[3];
     off3(L, ix, iy, iz, o);
     T* dd[3] = {d0, d1, d2};
@@ -434,9 +439,8 @@ __global__ void ns_adj_combine_kernel(const DevLayout L, const cplx<T>* mu, cons
   const int64_t total = static_cast<int64_t>(g.nx) * g.ny * g.nzh;
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int iz = static_cast<int>(t % g.nzh);
-    const int iy = static_cast<int>((t / g.nzh) % g.ny);
-    const int ix = static_cast<int>(t / (static_cast<int64_t>(g.nzh) * g.ny));
+    int ix, iy, iz;
+    decode_point(t, g.nzh, g.ny, &ix, &iy, &iz);
     const int mx = signed_mode(ix, g.nx), my = signed_mode(iy, g.ny), mz = iz;
     const bool keep = abs(mx) <= g.cx && abs(my) <= g.cy && mz <= g.cz;
     const double kx = mx * g.kscale, ky = my * g.kscale, kz = mz * g.kscale;

@@ -15,82 +15,16 @@
 // touch consecutive addresses for either row orientation); the passes in
 // between exchange values through padded shared memory (one pad element per
 // 256 bytes, which keeps the stride-R Stockham writes conflict-light).
-#include "fft_tile.cuh"
+#include "fft_fast.cuh"
 
 namespace dfft {
 namespace dev {
-
-using namespace radix;
-
-
-// B lines per CTA, N/V threads per line.
-// AFF: the general-layout variant (affine lines on the sides that set
-// src_line_affine / dst_line_affine); the separable variant carries none of
-// its code, which keeps its register count.
-// Resident CTAs per SM the register budget is sized for.  Left alone, the
-// compiler spends registers on scheduling freedom: the separable 8-value
-// kernels take a few more than the budget of their natural occupancy (b-fast
-// 1024-thread tiles lose half their resident threads at 33+ registers) and
-// the 24-value kernels anything up to 150.  So 8-value kernels are held to
-// 2048 (b-fast) or 1536 (a-fast) complex64 threads, or 1024 complex128
-// threads, per SM, and 24-value kernels to 768 complex64 or 384 complex128
-// threads (about 85 / 170 registers).  The general-layout 8-value variant
-// keeps the compiler's choice.
-template <typename T, int N, int THREADS, bool AFAST, bool AFF>
-struct MinBlocks {
-  static constexpr bool v8 = Vals<N>::value == 8;
-  static constexpr bool bound = !(v8 && AFF);
-  static constexpr int target = v8 ? (sizeof(T) == 4 ? (AFAST ? 1536 : 2048) : 1024) : (sizeof(T) == 4 ? 768 : 384);
-  static constexpr int v = target / THREADS;
-  static constexpr int value = (bound && v > 0) ? v : 1;
-};
-
-template <typename T, bool INV, int N, int B, bool AFAST, bool AFF>
-__global__ void __launch_bounds__(N / Vals<N>::value * B,
-                                  (MinBlocks<T, N, N / Vals<N>::value * B, AFAST, AFF>::value))
-    fft_fast_kernel(const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  // grid (tiles_b, Eo0, Eo1): tile along b, coordinates along o0 and o1
-  fast_tile<T, INV, N, B, AFAST, AFF>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
-}
-
-template <typename T, bool C2R, int N, int B, bool AFF>
-__global__ void __launch_bounds__(N / Vals<N>::value * B) fft_real_kernel(const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  // grid (tiles_b, Eo0, Eo1): tile along b, coordinates along o0 and o1
-  real_tile<T, C2R, N, B, AFF>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
-}
-
-// Default lines per CTA: at least 128-byte rows for b-fast tiles (16
-// complex64 or 8 complex128), at least 256 threads, at most 1024 threads
-// (N/V per line).  The launcher also has variants with 1/2 and 1/4 of it.
-template <typename T>
-constexpr int fast_lines(int n) {
-  const int tt = n % 3 == 0 ? n / 24 : n / 8;
-  const int rows = sizeof(T) == 4 ? 16 : 8;
-  const int want = rows > 256 / tt ? rows : 256 / tt;
-  const int cap = 1024 / tt;
-  return want < cap ? want : cap;
-}
-
-template <typename T, int N, bool INV, bool AF, int B, bool AFF = false>
-static cudaError_t launch_fast_b(const StageArgs& A, cudaStream_t st) {
-  constexpr int LP = SmemShape<T, N, B, AF>::LP;
-  const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
-  auto k = fft_fast_kernel<T, INV, N, B, AF, AFF>;
-  const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
-  if (e != cudaSuccess) return e;
-  k<<<fast_grid(A), N / Vals<N>::value * B, smem, st>>>(with_table_offsets(A));
-  return cudaGetLastError();
-}
 
 template <typename T, int N, bool INV, bool AF>
 static cudaError_t launch_fast_n(const StageArgs& A, cudaStream_t st) {
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
-  if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab || A.pre_mode)  // general layouts: default tile only
-    return A.B == B0 ? launch_fast_b<T, N, INV, AF, B0, true>(A, st) : cudaErrorInvalidValue;
   if (A.B == B0) return launch_fast_b<T, N, INV, AF, B0>(A, st);
   if (A.B == B1) return launch_fast_b<T, N, INV, AF, B1>(A, st);
   if (A.B == B2) return launch_fast_b<T, N, INV, AF, B2>(A, st);
@@ -105,24 +39,11 @@ static cudaError_t launch_fast_t(const StageArgs& A, bool inverse, bool afast, c
   return afast ? launch_fast_n<T, N, false, true>(A, st) : launch_fast_n<T, N, false, false>(A, st);
 }
 
-template <typename T, int N, bool C2R, int B, bool AFF = false>
-static cudaError_t launch_real_b(const StageArgs& A, cudaStream_t st) {
-  constexpr int LP = SmemShape<T, N, B, true>::LP;
-  const size_t smem = sizeof(cplx<T>) * (N + static_cast<size_t>(B) * LP);
-  auto k = fft_real_kernel<T, C2R, N, B, AFF>;
-  const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
-  if (e != cudaSuccess) return e;
-  k<<<fast_grid(A), N / Vals<N>::value * B, smem, st>>>(with_table_offsets(A));
-  return cudaGetLastError();
-}
-
 template <typename T, int N, bool C2R>
 static cudaError_t launch_real_n(const StageArgs& A, cudaStream_t st) {
   constexpr int B0 = fast_lines<T>(N);
   constexpr int B1 = B0 / 2 > 0 ? B0 / 2 : 1;
   constexpr int B2 = B0 / 4 > 0 ? B0 / 4 : 1;
-  if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab || A.pre_mode)
-    return A.B == B0 ? launch_real_b<T, N, C2R, B0, true>(A, st) : cudaErrorInvalidValue;
   if (A.B == B0) return launch_real_b<T, N, C2R, B0>(A, st);
   if (A.B == B1) return launch_real_b<T, N, C2R, B1>(A, st);
   if (A.B == B2) return launch_real_b<T, N, C2R, B2>(A, st);
@@ -147,6 +68,7 @@ bool fast_stage_supported(int n) {
 
 cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afast, cudaStream_t st) {
   if (A.Eo0 > fast_stage_max_grid_yz() || A.Eo1 > fast_stage_max_grid_yz()) return cudaErrorInvalidValue;
+  if (general_stage(A)) return launch_fast_general(A, dbl, inverse, afast, st);
 #define DFFT_CASE(N_)                                                                 \
   case N_:                                                                            \
     return dbl ? launch_fast_t<double, N_>(A, inverse, afast, st)                     \
@@ -174,6 +96,7 @@ cudaError_t launch_fft_fast(const StageArgs& A, bool dbl, bool inverse, bool afa
 
 cudaError_t launch_fft_fast_real(const StageArgs& A, bool dbl, bool c2r, cudaStream_t st) {
   if (A.Eo0 > fast_stage_max_grid_yz() || A.Eo1 > fast_stage_max_grid_yz()) return cudaErrorInvalidValue;
+  if (general_stage(A)) return launch_real_general(A, dbl, c2r, st);
 #define DFFT_CASE(N_)                                                                          \
   case N_:                                                                                     \
     if (dbl) return c2r ? launch_real_n<double, N_, true>(A, st) : launch_real_n<double, N_, false>(A, st); \

@@ -1299,8 +1299,7 @@ void Plan::autotune() {
     for (auto& op : *progs) {
       if (op.type != Op::Stage || !op.fast) continue;
       dev::StageArgs& A = op.sa;
-      if (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab)
-        continue;  // general-layout variant: default tile only
+
       // Trial buffers: the op's own plan-owned buffers, else the scratch
       // pair; each must hold the whole layout the stage reads / writes
       // (chirp-z stages run their FFTs on arrays larger than the scratch).
@@ -1320,7 +1319,9 @@ void Plan::autotune() {
       const bool tma_ok = op.tma.ok;                                    // eligible for the TMA-fed kernel
       k << "fast:n" << A.n << (d_.dbl ? "f64" : "f32") << (op.inverse ? "i" : "f") << (A.load_afast ? "a" : "b")
         << (op.kind == dev::kR2C ? "r2c" : op.kind == dev::kC2R ? "c2r" : "") << (pair_ok ? "P" : "")
-        << (tma_ok ? "T" : "") << (A.comp ? "C" : "") << ":" << A.Eb << "x" << A.Eo0 << "x" << A.Eo1;
+        << (tma_ok ? "T" : "") << (A.comp ? "C" : "")
+        << (A.src_line_affine || A.dst_line_affine || A.src_atab || A.dst_atab ? "G" : "") << ":" << A.Eb << "x"
+        << A.Eo0 << "x" << A.Eo1;
       // the topologies and line strides of both sides: stages of one shape
       // that read or write differently blocked layouts are tuned apart
       for (int side : {op.src_layout, op.dst_layout}) {
@@ -1536,10 +1537,11 @@ void Plan::execute_backward_premul(const void* in, void* out, const dev::StageAr
   const auto& prog = prog_[1];
   Op op = prog.front();
   dev::StageArgs A = op.sa;
-  // the one-line kernel, general-layout variant, default tile
+  // the one-line kernel, general-layout variant: the tuned tile of a
+  // one-line stage, else the default one
+  if (A.pairs) A.B = dev::fast_stage_lines(d_.dbl, A.n);
   A.pairs = 0;
   A.comp = 0;
-  A.B = dev::fast_stage_lines(d_.dbl, A.n);
   A.tiles_b = (A.Eb + A.B - 1) / A.B;
   op.tiles = static_cast<unsigned>(static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1);
   A.pre_mode = pre.pre_mode;

@@ -40,6 +40,7 @@ sys.path.insert(0, os.path.join(ROOT, "distributed-fft-for-kokkos_b200"))
 N_EDGE = 512
 TOPO_IN, TOPO_OUT = (4, 4, 1), (1, 4, 4)
 CPU_SAMPLE_EDGE = 256
+REF_BUDGET_S = 150.0
 WORKLOAD = (f"{N_EDGE}^3 C2C complex64 forward+backward, pencil {TOPO_IN}->{TOPO_OUT} "
             f"(16 virtual ranks on one GPU), fused")
 METRIC = "3D FFT fwd+bwd algorithmic HBM throughput"
@@ -119,18 +120,17 @@ def cpu_model():
     return "unknown"
 
 
-def cpu_baseline(steps=2, workers=None):
+def cpu_baseline(steps=2, workers=None, n=CPU_SAMPLE_EDGE):
     """CPU oracle (numpy restatement of the reference's block walk: pocketfft
     local FFTs on `workers` threads, pack / all-to-all / unpack) on a bounded
-    sample of the workload: the same pencil at 256^3.  The block list comes
-    from oracle/plans/ (precomputed planner output), so this leg loads no
-    product code."""
+    sample of the workload: the same pencil at n^3 (256^3 by default).  The
+    block list comes from oracle/plans/ (precomputed planner output), so this
+    leg loads no product code."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
 
     import dfft_oracle as O
 
-    n = CPU_SAMPLE_EDGE
     with open(os.path.join(ROOT, "oracle", "plans", f"c2c_{n}_pencil_441_144.json")) as f:
         info = json.load(f)["plan"]
     workers = workers or os.cpu_count() or 1
@@ -161,10 +161,16 @@ def run_reference(args):
     if rank != 0:
         return
     workers = os.cpu_count() or 1
-    cpu_baseline(steps=1, workers=workers)  # warm-up (imports, allocator)
+    # the sample edge: 256^3, halved while the timed steps would take more
+    # than REF_BUDGET_S of CPU time (the whole run stays within a few minutes)
+    edge = CPU_SAMPLE_EDGE
+    warm = cpu_baseline(steps=1, workers=workers, n=edge)  # warm-up (imports, allocator)
+    while edge > 64 and warm["ms_per_step"] / 1e3 * max(1, args.steps) > REF_BUDGET_S:
+        edge //= 2
+        warm = cpu_baseline(steps=1, workers=workers, n=edge)
     res = []
     for _ in range(max(1, args.steps)):
-        res.append(cpu_baseline(steps=1, workers=workers))
+        res.append(cpu_baseline(steps=1, workers=workers, n=edge))
     v = sorted(r["value"] for r in res)[len(res) // 2]
     cb = dict(res[0])
     cb["value"] = v

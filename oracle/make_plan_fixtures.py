@@ -17,8 +17,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 # (file name, global extents, in topology, out topology): the pencil of the
-# bench workload at the CPU sample size and at the workload size
-CONFIGS = [("c2c_256_pencil_441_144.json", (256, 256, 256), (4, 4, 1), (1, 4, 4)),
+# bench workload at the CPU sample sizes (256^3, and 128^3 / 64^3 when many
+# timed steps must fit the reference arm's time) and at the workload size
+CONFIGS = [("c2c_64_pencil_441_144.json", (64, 64, 64), (4, 4, 1), (1, 4, 4)),
+           ("c2c_128_pencil_441_144.json", (128, 128, 128), (4, 4, 1), (1, 4, 4)),
+           ("c2c_256_pencil_441_144.json", (256, 256, 256), (4, 4, 1), (1, 4, 4)),
            ("c2c_512_pencil_441_144.json", (512, 512, 512), (4, 4, 1), (1, 4, 4))]
 
 

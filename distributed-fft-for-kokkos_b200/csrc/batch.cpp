@@ -2,6 +2,7 @@
 #include "batch.hpp"
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <set>
@@ -20,8 +21,16 @@ bool batchable(const Op& op) {
   return dev::batch_stage_supported(op.sa.n);
 }
 
-// kind, inverse, a-fast rows, line length: one batched launch per group
-using GroupKey = std::tuple<int, bool, bool, int>;
+// kind, inverse, a-fast rows, line length, two-line tiles: one batched launch
+// per group
+using GroupKey = std::tuple<int, bool, bool, int, bool>;
+
+// complex64 C2C stages the one-tile launches would run two lines per thread
+// (separable sides, pair-aligned: op.single_B is set) take the batched
+// two-line tiles
+bool pair_batchable(const Op& op, bool dbl) {
+  return !dbl && op.kind == dev::kC2C && op.single_B != 0 && dev::batch_pair_lines(op.sa.n, op.sa.load_afast != 0) > 0;
+}
 
 void ck(cudaError_t e) {
   if (e != cudaSuccess) fail(kErrCuda, std::string("batch stream fork / join: ") + cudaGetErrorString(e));
@@ -81,7 +90,7 @@ std::size_t Batch::launches(bool forward) const {
       if (s >= prog.size() || prog[s].tiles == 0) continue;
       const Op& op = prog[s];
       if (batchable(op))
-        ++groups[GroupKey(op.kind, op.inverse, op.sa.load_afast != 0, op.sa.n)];
+        ++groups[GroupKey(op.kind, op.inverse, op.sa.load_afast != 0, op.sa.n, pair_batchable(op, dbl_))];
       else
         ++n;
     }
@@ -111,14 +120,18 @@ void Batch::execute(const void* const* ins, void* const* outs, bool forward, cud
         if (e != cudaSuccess) fail(kErrCuda, std::string("kernel launch failed: ") + cudaGetErrorString(e));
         continue;
       }
-      // the batched tile bodies: one line per thread group, lines per tile
-      // fixed by the line length
+      // the batched tile bodies: two lines per thread where the one-tile
+      // launch could run them, else one line per thread group; lines per
+      // tile fixed by the line length
+      // (b-fast pairs move 16 bytes at a time: both buffers on 16-byte boundaries)
+      const bool aligned = ((reinterpret_cast<std::uintptr_t>(A.in) | reinterpret_cast<std::uintptr_t>(A.out)) & 15) == 0;
+      const bool pair = pair_batchable(op, dbl_) && (A.load_afast || aligned);
       A.pairs = 0;
       A.comp = 0;
-      A.B = dev::batch_stage_lines(A.n);
+      A.B = pair ? dev::batch_pair_lines(A.n, A.load_afast != 0) : dev::batch_stage_lines(A.n);
       const int per = (op.kind == dev::kC2C) ? A.B : 2 * A.B;
       A.tiles_b = (A.Eb + per - 1) / per;
-      groups[GroupKey(op.kind, op.inverse, A.load_afast != 0, A.n)].push_back(A);
+      groups[GroupKey(op.kind, op.inverse, A.load_afast != 0, A.n, pair)].push_back(A);
     }
     // one launch per group (and per kMaxBatchFields fields of it); within a
     // launch the largest fields come first, so the last work items the
@@ -144,8 +157,10 @@ void Batch::execute(const void* const* ins, void* const* outs, bool forward, cud
           P.prefix[i + 1] = P.prefix[i] + tiles;
         }
         const cudaStream_t ls = lane(st, li);
-        const cudaError_t e = dev::launch_fft_batch(P, dbl_, std::get<0>(g.first), std::get<1>(g.first),
-                                                    std::get<2>(g.first), ls);
+        const cudaError_t e = std::get<4>(g.first)
+                                  ? dev::launch_fft_batch_pair(P, std::get<1>(g.first), std::get<2>(g.first), ls)
+                                  : dev::launch_fft_batch(P, dbl_, std::get<0>(g.first), std::get<1>(g.first),
+                                                          std::get<2>(g.first), ls);
         if (e != cudaSuccess) fail(kErrCuda, std::string("batched stage launch failed: ") + cudaGetErrorString(e));
       }
     }

@@ -155,6 +155,10 @@ cudaError_t launch_fft_pair_tma(const StageArgs& A, const void* map, const TmaCo
 // must have B = batch_stage_lines(n) (complex lines per tile) and the tiles_b
 // that goes with it; the args are taken by value (kernel parameter space).
 constexpr int kMaxBatchFields = 48;
+// Two-line variant (fft_batch_sep.cu): complex64 C2C stages of 2^k points
+// (16..2048) on separable sides whose line pairs start on 16-byte
+// boundaries; every field's StageArgs with B = batch_pair_lines(n, afast).
+int batch_pair_lines(int n, bool afast);
 struct BatchParams {
   int nfields;
   long long prefix[kMaxBatchFields + 1];
@@ -164,6 +168,7 @@ bool batch_stage_supported(int n);
 int batch_stage_lines(int n);
 // kind: kC2C, kR2C or kC2R (R2C / C2R: lines along a on both sides)
 cudaError_t launch_fft_batch(BatchParams& P, bool dbl, int kind, bool inverse, bool afast, cudaStream_t st);
+cudaError_t launch_fft_batch_pair(BatchParams& P, bool inverse, bool afast, cudaStream_t st);
 // Chirp-z (Bluestein) stage for line lengths the radix passes do not cover
 // (a prime factor above 13): X_k = c_k sum_j (x_j c_j) conj(c_{k-j}),
 // c_j = exp(-i pi j^2 / n) (conjugated for the inverse), as a circular

@@ -6,6 +6,7 @@
 
 #include <cstring>
 
+#include "fft_pair.cuh"
 #include "fft_tile.cuh"
 
 namespace dfft {
@@ -85,6 +86,34 @@ __global__ void __launch_bounds__(kBatchThreads, (BatchMinBlocks<T, N, true, AFF
   }
 }
 
+// Two-line (complex64, separable, 2^k points) batched C2C stage: the tile
+// body of fft_pair_kernel with its default pairs per tile, N/8 threads per
+// pair, at that kernel's register budget (1024 resident threads per SM).
+template <int N, bool AFAST>
+struct BatchPairs {
+  static constexpr int value = pair_option(N, AFAST, 0);
+  static constexpr int threads = N / 8 * value;
+  static constexpr int min_blocks = 1024 / threads > 0 ? 1024 / threads : 1;
+};
+
+template <bool INV, bool AFAST, int N>
+__global__ void __launch_bounds__(BatchPairs<N, AFAST>::threads, (BatchPairs<N, AFAST>::min_blocks))
+    fft_batch_pair_kernel(const __grid_constant__ BatchParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long long total = P.prefix[P.nfields];
+  int f = 0;
+  bool first = true;
+  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
+    while (w >= P.prefix[f + 1]) ++f;
+    const StageArgs& A = P.f[f];
+    int tb, co0, co1;
+    decode(A, static_cast<unsigned>(w - P.prefix[f]), &tb, &co0, &co1);
+    pair_tile<INV, N, BatchPairs<N, AFAST>::value, AFAST>(A, tb, co0, co1, smem_raw, first);
+    first = false;
+    __syncthreads();
+  }
+}
+
 template <typename T>
 size_t tile_smem(int n, bool afast) {
   switch (n) {
@@ -99,21 +128,28 @@ size_t tile_smem(int n, bool afast) {
   }
 }
 
-template <typename K>
+template <int THREADS = kBatchThreads, typename K>
 cudaError_t launch_persistent(K kernel, BatchParams& P, size_t smem, cudaStream_t st) {
   cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kernel), smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0, per_sm = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBatchThreads, smem)) != cudaSuccess)
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, THREADS, smem)) != cudaSuccess)
     return e;
   long long grid = static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1);
   const long long total = P.prefix[P.nfields];
   if (grid > total) grid = total;
   if (grid < 1) return cudaSuccess;
-  kernel<<<static_cast<unsigned>(grid), kBatchThreads, smem, st>>>(P);
+  kernel<<<static_cast<unsigned>(grid), THREADS, smem, st>>>(P);
   return cudaGetLastError();
+}
+
+template <bool INV, bool AFAST, int N>
+cudaError_t launch_batch_pair_n(BatchParams& P, cudaStream_t st) {
+  constexpr size_t smem = pair_tile_smem<N, BatchPairs<N, AFAST>::value, AFAST>();
+  for (int i = 0; i < P.nfields; ++i) P.f[i] = with_table_offsets(P.f[i]);
+  return launch_persistent<BatchPairs<N, AFAST>::threads>(fft_batch_pair_kernel<INV, AFAST, N>, P, smem, st);
 }
 
 template <typename T, bool AFF, int N>

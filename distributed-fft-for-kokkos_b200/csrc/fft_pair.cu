@@ -35,53 +35,9 @@ struct PairMinBlocks {
 template <bool INV, int N, int PB, bool AFAST, bool COMP = false>
 __global__ void __launch_bounds__(N / 8 * PB, (PairMinBlocks<N / 8 * PB, COMP>::value))
     fft_pair_kernel(const StageArgs A) {
-  using C = float2;
-  constexpr int V = 8;
-  static_assert(Vals<N>::value == V, "two-line kernel: lines of 2^k points");
-  constexpr int TT = N / V;
-  using SH = SmemShape<double, N, PB, AFAST>;  // 16-byte elements: the complex128 line layout
-  constexpr int LP = SH::LP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tw = reinterpret_cast<C*>(smem_raw);
-  float4* tile = reinterpret_cast<float4*>(smem_raw + sizeof(C) * N);
-  const DevLayout ls = A.src, ld = A.dst;
-
   // grid (tiles_b, Eo0, Eo1)
-  const int b0 = blockIdx.x * 2 * PB, co0 = blockIdx.y, co1 = blockIdx.z;
-  const int nb = min(2 * PB, A.Eb - b0);
-  int lp, t;
-  if (AFAST) {
-    t = threadIdx.x % TT;
-    lp = threadIdx.x / TT;
-  } else {
-    lp = threadIdx.x % PB;
-    t = threadIdx.x / PB;
-  }
-  const int l0 = AFAST ? lp : 2 * lp, l1 = AFAST ? lp + PB : 2 * lp + 1;
-  const bool act0 = l0 < nb, act1 = l1 < nb;
-
-  {
-    const C* gtw = reinterpret_cast<const C*>(A.tw);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
-  }
-  int64_t so = A.src_abase, dof = A.dst_abase;
-  if (A.o0 >= 0) {
-    so += __ldg(ls.t + A.s_to0 + co0);
-    dof += __ldg(ld.t + A.d_to0 + co0);
-  }
-  if (A.o1 >= 0) {
-    so += __ldg(ls.t + A.s_to1 + co1);
-    dof += __ldg(ld.t + A.d_to1 + co1);
-  }
-
-  C v0[V], v1[V];
-  const C* in = reinterpret_cast<const C*>(A.in);
-  load_pair<N, AFAST>(A, in, so, b0, l0, l1, act0, act1, t, v0, v1);
-  __syncthreads();  // twiddles staged
-
-  run_fft_pair<INV, N, 0, TT, SH::S, COMP>(v0, v1, t, tw, tile + lp * LP);
-
-  store_pair<N, AFAST>(A, reinterpret_cast<C*>(A.out), dof, b0, l0, l1, act0, act1, t, v0, v1);
+  pair_tile<INV, N, PB, AFAST, COMP>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 // Streaming variant: a CTA walks A.tpc consecutive tiles along b (grid

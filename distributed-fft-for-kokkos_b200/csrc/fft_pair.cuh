@@ -159,6 +159,66 @@ __device__ __forceinline__ void store_pair(const StageArgs& A, float2* out, int6
   }
 }
 
+// One tile (tile tb along b, coordinates co0 / co1) of a two-line C2C stage:
+// PB line pairs, N/8 threads per pair, `smem_raw` holding N complex64
+// twiddles and PB * LP 16-byte line elements (pair_tile_smem).  Called by
+// fft_pair_kernel (one tile per CTA) and by the batched stage kernels, whose
+// CTAs walk tiles of many fields (stage_tw = false: the twiddles of this N
+// are already staged).  Separable sides only.
+template <bool INV, int N, int PB, bool AFAST, bool COMP = false>
+__device__ __forceinline__ void pair_tile(const StageArgs& A, int tb, int co0, int co1, unsigned char* smem_raw,
+                                          bool stage_tw = true) {
+  using C = float2;
+  constexpr int V = 8;
+  static_assert(Vals<N>::value == V, "two-line kernel: lines of 2^k points");
+  constexpr int TT = N / V;
+  using SH = SmemShape<double, N, PB, AFAST>;  // 16-byte elements: the complex128 line layout
+  constexpr int LP = SH::LP;
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  float4* tile = reinterpret_cast<float4*>(smem_raw + sizeof(C) * N);
+  const DevLayout ls = A.src, ld = A.dst;
+
+  const int b0 = tb * 2 * PB;
+  const int nb = min(2 * PB, A.Eb - b0);
+  int lp, t;
+  if (AFAST) {
+    t = threadIdx.x % TT;
+    lp = threadIdx.x / TT;
+  } else {
+    lp = threadIdx.x % PB;
+    t = threadIdx.x / PB;
+  }
+  const int l0 = AFAST ? lp : 2 * lp, l1 = AFAST ? lp + PB : 2 * lp + 1;
+  const bool act0 = l0 < nb, act1 = l1 < nb;
+
+  if (stage_tw) {
+    const C* gtw = reinterpret_cast<const C*>(A.tw);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  }
+  int64_t so = A.src_abase, dof = A.dst_abase;
+  if (A.o0 >= 0) {
+    so += __ldg(ls.t + A.s_to0 + co0);
+    dof += __ldg(ld.t + A.d_to0 + co0);
+  }
+  if (A.o1 >= 0) {
+    so += __ldg(ls.t + A.s_to1 + co1);
+    dof += __ldg(ld.t + A.d_to1 + co1);
+  }
+
+  C v0[V], v1[V];
+  const C* in = reinterpret_cast<const C*>(A.in);
+  load_pair<N, AFAST>(A, in, so, b0, l0, l1, act0, act1, t, v0, v1);
+  __syncthreads();  // twiddles staged
+
+  run_fft_pair<INV, N, 0, TT, SH::S, COMP>(v0, v1, t, tw, tile + lp * LP);
+
+  store_pair<N, AFAST>(A, reinterpret_cast<C*>(A.out), dof, b0, l0, l1, act0, act1, t, v0, v1);
+}
+
+template <int N, int PB, bool AFAST>
+constexpr size_t pair_tile_smem() {
+  return sizeof(float2) * N + sizeof(float4) * static_cast<size_t>(PB) * SmemShape<double, N, PB, AFAST>::LP;
+}
 
 // Line pairs per CTA, option i (0 default, 1 half, 2 double or quarter):
 //   b-fast: 8 pairs (16-line, 128-byte rows) or enough for 256 threads;

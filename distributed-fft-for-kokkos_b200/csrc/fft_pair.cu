@@ -32,12 +32,12 @@ struct PairMinBlocks {
 
 // PB line pairs per CTA (2 PB lines), N/8 threads per pair.  COMP: the last
 // radix pass in compensated arithmetic (compute_pass_comp).
-template <bool INV, int N, int PB, bool AFAST, bool COMP = false>
+template <bool INV, int N, int PB, bool AFAST, bool COMP = false, bool ATAB = false>
 __global__ void __launch_bounds__(N / 8 * PB, (PairMinBlocks<N / 8 * PB, COMP>::value))
     fft_pair_kernel(const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // grid (tiles_b, Eo0, Eo1)
-  pair_tile<INV, N, PB, AFAST, COMP>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+  pair_tile<INV, N, PB, AFAST, COMP, ATAB>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 // Streaming variant: a CTA walks A.tpc consecutive tiles along b (grid
@@ -106,14 +106,14 @@ __global__ void __launch_bounds__(N / 8 * PB, 1) fft_pair_stream_kernel(const St
   }
 }
 
-template <int N, bool INV, bool AF, int PB, bool COMP = false>
+template <int N, bool INV, bool AF, int PB, bool COMP = false, bool ATAB = false>
 static cudaError_t launch_pair_b(const StageArgs& A, cudaStream_t st) {
   if constexpr (PB <= 0) {
     return cudaErrorInvalidValue;
   } else {
     constexpr int LP = SmemShape<double, N, PB, AF>::LP;
     const size_t smem = sizeof(float2) * N + sizeof(float4) * static_cast<size_t>(PB) * LP;
-    auto k = fft_pair_kernel<INV, N, PB, AF, COMP>;
+    auto k = fft_pair_kernel<INV, N, PB, AF, COMP, ATAB>;
     const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     k<<<fast_grid(A), N / 8 * PB, smem, st>>>(with_table_offsets(A));
@@ -139,6 +139,13 @@ static cudaError_t launch_pair_stream(const StageArgs& A, cudaStream_t st) {
 template <int N, bool INV, bool AF>
 static cudaError_t launch_pair_n(const StageArgs& A, cudaStream_t st) {
   constexpr int P0 = pair_option(N, AF, 0), P1 = pair_option(N, AF, 1), P2 = pair_option(N, AF, 2);
+  if (A.src_atab || A.dst_atab) {
+    // a-fast sides read through the axis table: the default tile, plain FP32
+    if constexpr (AF) {
+      if (!A.comp && A.B == 2 * P0) return launch_pair_b<N, INV, AF, P0, false, true>(A, st);
+    }
+    return cudaErrorInvalidValue;
+  }
   if (A.comp) return A.B == 2 * P0 ? launch_pair_b<N, INV, AF, P0, true>(A, st) : cudaErrorInvalidValue;
   if (A.B == 2 * P0) return launch_pair_b<N, INV, AF, P0>(A, st);
   if (P1 > 0 && A.B == 2 * P1) return launch_pair_b<N, INV, AF, P1>(A, st);
@@ -149,7 +156,7 @@ static cudaError_t launch_pair_n(const StageArgs& A, cudaStream_t st) {
 template <int N>
 static cudaError_t launch_pair_t(const StageArgs& A, bool inverse, bool afast, cudaStream_t st) {
   if (A.pairs == 2) {
-    if (A.comp) return cudaErrorInvalidValue;
+    if (A.comp || A.src_atab || A.dst_atab) return cudaErrorInvalidValue;
     if (inverse) return afast ? launch_pair_stream<N, true, true>(A, st) : launch_pair_stream<N, true, false>(A, st);
     return afast ? launch_pair_stream<N, false, true>(A, st) : launch_pair_stream<N, false, false>(A, st);
   }

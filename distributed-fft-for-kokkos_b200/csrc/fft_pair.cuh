@@ -62,7 +62,9 @@ __device__ __forceinline__ void run_fft_pair(float2* v0, float2* v1, int t, cons
 // Loads the pair (l0, l1) of one tile (first line b0) into v0 / v1.
 // b-fast: positions p of the pair at (line l0 offset) + p * stride; stride and
 // offsets are even (host check) and (N - 1) * stride < 2^31.
-template <int N, bool AFAST>
+// ATAB (a-fast only): a side whose offsets along a come from the axis table
+// (an exchange buffer cut into bins along a; StageArgs::src_atab / dst_atab).
+template <int N, bool AFAST, bool ATAB = false>
 __device__ __forceinline__ void load_pair(const StageArgs& A, const float2* in, int64_t so, int b0, int l0, int l1,
                                           bool act0, bool act1, int t, float2* v0, float2* v1) {
   using C = float2;
@@ -77,7 +79,8 @@ __device__ __forceinline__ void load_pair(const StageArgs& A, const float2* in, 
     for (int q = 0; q < Q0; ++q)
 #pragma unroll
       for (int r = 0; r < R0; ++r) {
-        const int p = in_pos<N, 0, TT>(t, q, r);
+        const int pos = in_pos<N, 0, TT>(t, q, r);
+        const int64_t p = (ATAB && A.src_atab) ? __ldg(ls.t + A.s_ta + pos) : pos;
         v0[q * R0 + r] = act0 ? row0[p] : zero;
         v1[q * R0 + r] = act1 ? row1[p] : zero;
       }
@@ -109,7 +112,7 @@ __device__ __forceinline__ void load_pair(const StageArgs& A, const float2* in, 
 }
 
 // Scales (when the stage scales) and stores the pair after the last pass.
-template <int N, bool AFAST>
+template <int N, bool AFAST, bool ATAB = false>
 __device__ __forceinline__ void store_pair(const StageArgs& A, float2* out, int64_t dof, int b0, int l0, int l1,
                                            bool act0, bool act1, int t, float2* v0, float2* v1) {
   using C = float2;
@@ -132,7 +135,8 @@ __device__ __forceinline__ void store_pair(const StageArgs& A, float2* out, int6
     for (int q = 0; q < QL; ++q)
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
-        const int p = t + last_rel<N, TT>(q, r);
+        const int pos = t + last_rel<N, TT>(q, r);
+        const int64_t p = (ATAB && A.dst_atab) ? __ldg(ld.t + A.d_ta + pos) : pos;
         if (act0) row0[p] = v0[q * RL + r];
         if (act1) row1[p] = v1[q * RL + r];
       }
@@ -165,7 +169,7 @@ __device__ __forceinline__ void store_pair(const StageArgs& A, float2* out, int6
 // fft_pair_kernel (one tile per CTA) and by the batched stage kernels, whose
 // CTAs walk tiles of many fields (stage_tw = false: the twiddles of this N
 // are already staged).  Separable sides only.
-template <bool INV, int N, int PB, bool AFAST, bool COMP = false>
+template <bool INV, int N, int PB, bool AFAST, bool COMP = false, bool ATAB = false>
 __device__ __forceinline__ void pair_tile(const StageArgs& A, int tb, int co0, int co1, unsigned char* smem_raw,
                                           bool stage_tw = true) {
   using C = float2;
@@ -207,12 +211,12 @@ __device__ __forceinline__ void pair_tile(const StageArgs& A, int tb, int co0, i
 
   C v0[V], v1[V];
   const C* in = reinterpret_cast<const C*>(A.in);
-  load_pair<N, AFAST>(A, in, so, b0, l0, l1, act0, act1, t, v0, v1);
+  load_pair<N, AFAST, ATAB>(A, in, so, b0, l0, l1, act0, act1, t, v0, v1);
   __syncthreads();  // twiddles staged
 
   run_fft_pair<INV, N, 0, TT, SH::S, COMP>(v0, v1, t, tw, tile + lp * LP);
 
-  store_pair<N, AFAST>(A, reinterpret_cast<C*>(A.out), dof, b0, l0, l1, act0, act1, t, v0, v1);
+  store_pair<N, AFAST, ATAB>(A, reinterpret_cast<C*>(A.out), dof, b0, l0, l1, act0, act1, t, v0, v1);
 }
 
 template <int N, int PB, bool AFAST>

@@ -693,8 +693,11 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
       }
       return true;
     };
+    // (axis-table sides: a-fast rows only, which the two-line kernel reads as
+    // plain rows except for the positions along a)
+    const bool atab = satab || datab;
     if (kind == dev::kC2C && !d_.dbl && dev::pair_stage_supported(static_cast<int>(n)) && !saff && !daff &&
-        !satab && !datab &&
+        (!atab || A.load_afast) &&
         (A.load_afast || (pair_aligned(src_l, sab, sas) && pair_aligned(dst_l, dab, das)))) {
       int opts[3];
       dev::pair_stage_line_options(static_cast<int>(n), A.load_afast != 0, opts);
@@ -712,7 +715,8 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
         A.tiles_b = static_cast<int>((Dl.gext[b] + tl - 1) / tl);
       }
       // compensated last pass: the default tiles of the two kernels above
-      if (d_.comp) A.comp = 1;
+      // (not on axis-table sides: plain FP32 there)
+      if (d_.comp && !atab) A.comp = 1;
     }
     const unsigned long long ft = static_cast<unsigned long long>(A.tiles_b) * A.Eo0 * A.Eo1;
     if (ft >= (1ull << 31)) fail(kErrUnsupported, "too many tiles");
@@ -1373,7 +1377,12 @@ void Plan::autotune() {
         for (int i = 0; i < nt; ++i)
           if (!op.tma.b_split || op.tma.lb % static_cast<std::uint64_t>(opts[i]) == 0) cand.push_back(kTmaCode + opts[i]);
       }
-      if (pair_ok && !A.comp) {
+      const bool atab = A.src_atab || A.dst_atab;
+      if (pair_ok && !A.comp && atab) {
+        // axis-table sides: the two-line kernel's default tile only
+        dev::pair_stage_line_options(A.n, A.load_afast != 0, opts);
+        cand.push_back(kPairCode + opts[0]);
+      } else if (pair_ok && !A.comp) {
         const int np = dev::pair_stage_line_options(A.n, A.load_afast != 0, opts);
         for (int i = 0; i < np; ++i) cand.push_back(kPairCode + opts[i]);
         const int sb = dev::pair_stage_stream_lines(A.n, A.load_afast != 0);

@@ -140,10 +140,8 @@ template <int N, bool INV, bool AF>
 static cudaError_t launch_pair_n(const StageArgs& A, cudaStream_t st) {
   constexpr int P0 = pair_option(N, AF, 0), P1 = pair_option(N, AF, 1), P2 = pair_option(N, AF, 2);
   if (A.src_atab || A.dst_atab) {
-    // a-fast sides read through the axis table: the default tile, plain FP32
-    if constexpr (AF) {
-      if (!A.comp && A.B == 2 * P0) return launch_pair_b<N, INV, AF, P0, false, true>(A, st);
-    }
+    // sides read or written through the axis table: the default tile, plain FP32
+    if (!A.comp && A.B == 2 * P0) return launch_pair_b<N, INV, AF, P0, false, true>(A, st);
     return cudaErrorInvalidValue;
   }
   if (A.comp) return A.B == 2 * P0 ? launch_pair_b<N, INV, AF, P0, true>(A, st) : cudaErrorInvalidValue;

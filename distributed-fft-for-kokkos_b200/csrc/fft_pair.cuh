@@ -62,8 +62,8 @@ __device__ __forceinline__ void run_fft_pair(float2* v0, float2* v1, int t, cons
 // Loads the pair (l0, l1) of one tile (first line b0) into v0 / v1.
 // b-fast: positions p of the pair at (line l0 offset) + p * stride; stride and
 // offsets are even (host check) and (N - 1) * stride < 2^31.
-// ATAB (a-fast only): a side whose offsets along a come from the axis table
-// (an exchange buffer cut into bins along a; StageArgs::src_atab / dst_atab).
+// ATAB: a side whose offsets along a come from the axis table (an exchange
+// buffer cut into bins along a; StageArgs::src_atab / dst_atab).
 template <int N, bool AFAST, bool ATAB = false>
 __device__ __forceinline__ void load_pair(const StageArgs& A, const float2* in, int64_t so, int b0, int l0, int l1,
                                           bool act0, bool act1, int t, float2* v0, float2* v1) {
@@ -83,6 +83,24 @@ __device__ __forceinline__ void load_pair(const StageArgs& A, const float2* in, 
         const int64_t p = (ATAB && A.src_atab) ? __ldg(ls.t + A.s_ta + pos) : pos;
         v0[q * R0 + r] = act0 ? row0[p] : zero;
         v1[q * R0 + r] = act1 ? row1[p] : zero;
+      }
+  } else if (ATAB && A.src_atab) {
+    // b-fast pair rows at the axis-table offsets of their positions (even,
+    // host check: 16-byte aligned pairs)
+    const C* line = in + so + (act0 ? __ldg(ls.t + A.s_tb + b0 + l0) : 0);
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int64_t o = __ldg(ls.t + A.s_ta + in_pos<N, 0, TT>(t, q, r));
+        if (act1) {
+          const float4 w = *reinterpret_cast<const float4*>(line + o);
+          v0[q * R0 + r] = make_float2(w.x, w.y);
+          v1[q * R0 + r] = make_float2(w.z, w.w);
+        } else {
+          v0[q * R0 + r] = act0 ? line[o] : zero;
+          v1[q * R0 + r] = zero;
+        }
       }
   } else {
     const int st = static_cast<int>(A.src_astride);
@@ -139,6 +157,20 @@ __device__ __forceinline__ void store_pair(const StageArgs& A, float2* out, int6
         const int64_t p = (ATAB && A.dst_atab) ? __ldg(ld.t + A.d_ta + pos) : pos;
         if (act0) row0[p] = v0[q * RL + r];
         if (act1) row1[p] = v1[q * RL + r];
+      }
+  } else if (ATAB && A.dst_atab) {
+    if (!act0) return;
+    C* line = out + dof + __ldg(ld.t + A.d_tb + b0 + l0);
+#pragma unroll
+    for (int q = 0; q < QL; ++q)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int64_t o = __ldg(ld.t + A.d_ta + t + last_rel<N, TT>(q, r));
+        const C a = v0[q * RL + r], b = v1[q * RL + r];
+        if (act1)
+          *reinterpret_cast<float4*>(line + o) = make_float4(a.x, a.y, b.x, b.y);
+        else
+          line[o] = a;
       }
   } else if (act0) {
     const int st = static_cast<int>(A.dst_astride);

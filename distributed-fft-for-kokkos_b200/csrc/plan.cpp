@@ -678,9 +678,16 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
     // Two complex64 lines per thread: C2C of 2^k points on separable sides;
     // b-fast tiles move both lines of a pair with one 16-byte access, so
     // every pair must start on an even element on both sides.
-    auto pair_aligned = [&](int l, std::int64_t abase, std::int64_t astride) {
+    auto pair_aligned = [&](int l, std::int64_t abase, std::int64_t astride, bool atab) {
       const LayoutTables& T = tables_[l];
-      if (T.mode != 0 || (abase & 1) || (astride & 1)) return false;
+      if (T.mode != 0) return false;
+      if (atab) {
+        const std::int64_t* oa = T.data.data() + T.off[a];
+        for (std::size_t c = 0; c < layouts_[l].gext[a]; ++c)
+          if (oa[c] & 1) return false;
+      } else if ((abase & 1) || (astride & 1)) {
+        return false;
+      }
       const std::int64_t* ob = T.data.data() + T.off[b];
       for (std::size_t c = 0; c + 1 < static_cast<std::size_t>(A.Eb); c += 2)
         if ((ob[c] & 1) || ob[c + 1] != ob[c] + 1) return false;
@@ -693,12 +700,11 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
       }
       return true;
     };
-    // (axis-table sides: a-fast rows only, which the two-line kernel reads as
-    // plain rows except for the positions along a)
+    // (axis-table sides: the two-line kernel takes the positions along a from
+    // the table; b-fast pairs need every offset even)
     const bool atab = satab || datab;
     if (kind == dev::kC2C && !d_.dbl && dev::pair_stage_supported(static_cast<int>(n)) && !saff && !daff &&
-        (!atab || A.load_afast) &&
-        (A.load_afast || (pair_aligned(src_l, sab, sas) && pair_aligned(dst_l, dab, das)))) {
+        (A.load_afast || (pair_aligned(src_l, sab, sas, satab) && pair_aligned(dst_l, dab, das, datab)))) {
       int opts[3];
       dev::pair_stage_line_options(static_cast<int>(n), A.load_afast != 0, opts);
       op.single_B = A.B;
@@ -708,7 +714,8 @@ Op Plan::make_stage(int src_l, int dst_l, std::size_t a, int kind, bool inverse,
       // b-fast source tiles moved by TMA when a tensor map can describe the
       // source layout (the default; the tuner may pick another variant)
       const int tl = dev::pair_tma_lines(static_cast<int>(n));
-      if (!A.load_afast && tl > 0 && tma_source(src_l, A, &op.tma) && (!op.tma.b_split || op.tma.lb % tl == 0)) {
+      if (!A.load_afast && tl > 0 && !atab && tma_source(src_l, A, &op.tma) &&
+          (!op.tma.b_split || op.tma.lb % tl == 0)) {
         op.pair_B = A.B;
         A.pairs = 3;
         A.B = tl;

@@ -8,8 +8,10 @@
   FP32 on the FP32-rounded inputs), the send buffers each rank's last stage
   wrote against the oracle's pack of the same rank (same tolerance, padding
   exactly zero), and the backward transform back to the input.
-* Two processes sharing the GPU run DistributedPlan over a gloo group
-  (buffers staged through host memory; no kernel waits on the other process),
+* Two processes (slab plans) and four processes (pencil plans: the row /
+  column sub-communicators) sharing the GPU run DistributedPlan over gloo
+  groups (buffers staged through host memory; no kernel waits on another
+  process),
   through both the Python segment loop and the C driver with the exchange
   callback (dfft_execute_exchanged): outputs against the oracle, received
   buffers bit for bit the all-to-all permutation of the sent ones."""
@@ -118,3 +120,11 @@ def test_distributed_plan_two_processes_on_one_gpu(tmp_path):
     cases = CASES2[:3] + [_case((32, 24, 20), (0, 1, 2), (2, 1, 1), (1, 2, 1), True)]
     run_processes(2, cases, tmp_path, "gpu")
     check_process_results(cases, tmp_path, 2, 1e-12, check_exchanged=True)
+
+
+def test_distributed_plan_four_processes_pencil_on_one_gpu(tmp_path):
+    # pencil topologies: row / column sub-communicators created by the plan,
+    # the library's CUDA segments between the exchanges
+    cases = [CASES4[0], CASES4[3], _case((32, 24, 20), (0, 1, 2), (2, 2, 1), (1, 2, 2), True)]
+    run_processes(4, cases, tmp_path, "gpu")
+    check_process_results(cases, tmp_path, 4, 1e-12, check_exchanged=True)
